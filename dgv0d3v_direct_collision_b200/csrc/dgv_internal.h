@@ -1,0 +1,136 @@
+// dgv_internal.h -- context, device layout and kernel entry points shared by
+// the sources of libdgv_b200.so.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/dgv_b200.h"
+
+namespace dgv {
+
+// One cell-pair block of the pair layout.  Records of the reference are
+// regrouped by the (canonical-frame) cells c1 <= c2 of their two velocities;
+// for an output cell D the block contributes iff both shifted cells
+// c1 + D - ccell and c2 + D - ccell stay inside the grid, i.e. iff D lies in
+// the box [lo, hi] (per axis).  This is the per-record bounds test of
+// collision_mod.f90:196-211 hoisted to the block.
+struct __align__(16) BlockInfo {
+    long long start;   // first pair of the block
+    int count;         // pairs in the block
+    int c1, c2;        // linear cell indices, canonical frame
+    signed char lo[3]; // valid output-cell box, inclusive
+    signed char hi[3];
+    short pad;
+};
+static_assert(sizeof(BlockInfo) == 32, "BlockInfo layout");
+
+// Host-side grid (own restatement of the reference's uniform mesh).
+struct Grid {
+    dgv_grid_desc d;
+    int P = 0, Nc = 0;
+    long long N = 0;
+    int ccell = -1, ccu = 0, ccv = 0, ccw = 0;
+    std::vector<double> gu, gv, gw;          // 1-D grids
+    std::vector<double> xu, wu, xv, wv, xw, ww;  // Gauss-Legendre rules
+    std::vector<double> lu, ru, lv, rv, lw, rw;  // cell bounds
+    std::vector<double> nu, nv, nw, nwt;     // node coordinates and weights
+    int cell_u(int c) const { return c / (d.Mv * d.Mw); }
+    int cell_v(int c) const { return (c / d.Mw) % d.Mv; }
+    int cell_w(int c) const { return c % d.Mw; }
+};
+int build_grid(const dgv_grid_desc &d, Grid &g, std::string &err);
+
+// Device copy of the A-arrays in the pair layout.
+//   rows64[pair] = { int32 o1, int32 o2, double v[P], pad }  (RD64 doubles)
+//   rows32[pair] = { int32 o1, int32 o2, float v[P], pad }   (RW32 words)
+// o1 = l1*Nc + (c1 - ccell), o2 = l2*Nc + (c2 - ccell): for output cell D the
+// two factors are f_s[o1 + D] and f_s[o2 + D] in the local-major shared copy
+// f_s[l*Nc + cell] of f.  v[p] is the A value of canonical basis function p
+// for the pair (0 where the reference has no record).
+struct Layout {
+    long long nrecords = 0, npairs = 0, nblocks = 0;
+    double record_shifts = 0;  // sum over records of valid shifts
+    int RD64 = 0, RW32 = 0;    // row length in doubles / 32-bit words
+    BlockInfo *blk = nullptr;  // device
+    void *rows64 = nullptr;    // device
+    void *rows32 = nullptr;    // device
+    std::vector<BlockInfo> h_blk;     // host copy
+    std::vector<double> h_work;       // per block: pairs x valid shifts
+    // work partitions: nchunks -> device array of nchunks+1 block bounds
+    std::map<int, int *> chunks;
+};
+void free_layout(Layout &L);
+
+struct Ctx {
+    int device = 0;
+    Grid grid;
+    Layout lay;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    bool async = false;
+    bool project = false;
+    int nchunks_opt = 0;
+    std::string err;
+    // device copies of node tables
+    double *d_nu = nullptr, *d_nv = nullptr, *d_nw = nullptr, *d_nwt = nullptr;
+    double gram_inv[25];  // inverse Gram matrix of the invariants, FP64
+    // device work buffers (grown on demand)
+    double *d_partial = nullptr;
+    size_t partial_bytes = 0;
+    double *d_in = nullptr, *d_out = nullptr;  // staging for host pointers
+    size_t in_bytes = 0, out_bytes = 0;
+    double *d_tmp[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t tmp_n = 0;
+    double *d_red = nullptr;  // reduction scratch
+    size_t red_bytes = 0;
+    // Adams-Bashforth history: right sides frhs1..frhs5 (newest first)
+    double *d_hist[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int ab_order = 0;
+    // linearisation point
+    double *d_fm = nullptr;
+    // autotuned chunk counts keyed by (precision, nvdf bucket)
+    std::map<long long, int> tuned;
+};
+
+// error helpers
+int set_err(Ctx *c, int code, const std::string &msg);
+#define DGV_CUDA(c, call)                                                        \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess)                                                   \
+            return dgv::set_err((c), DGV_ECUDA,                                  \
+                                std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int ensure_buffer(Ctx *c, double **p, size_t *have, size_t need_bytes);
+void release_graphs(const Ctx *c);
+
+// layout construction
+int layout_from_reference(Ctx *c, long long nnz, const int32_t *capphi, const double *A,
+                          const int32_t *xi, const int32_t *xi1, int one_based);
+int layout_synthetic(Ctx *c, unsigned long long seed, double Trad, int support_mode);
+int layout_export(Ctx *c, long long *nnz_out, int32_t *capphi, double *A, int32_t *xi,
+                  int32_t *xi1);
+int get_chunks(Ctx *c, int nchunks, int **d_bounds);
+
+// kernels (device pointers, ctx stream)
+int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision,
+                   double scale);
+int jvp_device(Ctx *c, const double *d_f, const double *d_df, double *d_q, int precision);
+int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int precision);
+int moments_device(Ctx *c, const double *d_f, int nvdf, double *h_out);
+int project_device(Ctx *c, double *d_q, int nvdf);
+int maxwellian_device(Ctx *c, double T, double u0, double v0, double w0, double n, double *d_f);
+int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, int precision);
+int ab_prepare_device(Ctx *c, double *d_f, double dt, int order, int precision);
+int ab_step_device(Ctx *c, double *d_f, double dt, int precision);
+
+}  // namespace dgv
+
+struct dgv_ctx {
+    dgv::Ctx c;
+};

@@ -1,0 +1,239 @@
+"""Host-side mirror of the reference's collision/time-stepping interface.
+
+`DGVSolver` wraps one C-ABI context (include/dgv_b200.h).  Its methods carry the
+names of the Fortran routines they replace, take the same arguments (minus the
+module globals, which live in the context) and fail the way the reference
+fails -- by raising instead of `stop`:
+
+    EvalCollisionPeriodicAPlus_DGV(f)        collision_mod.f90:143-229
+    EvalCollisionPeriodicMixedTermsA_DGV(f, fm)  collision_mod.f90:244-332
+    PrepareFMA_DGV(fm) / EvalCollisionLinear(f)  collision_mod.f90:377-464, 346-359
+    SpatialOperSH_DGV(f, dt)                 spat_oper_mod.f90:28-68 (run_mode 0)
+    TimeIntegratorORK_SH_DGV(f, dt)          time_integr_mod.f90:26-152
+    PrepareMTS_SH_DGV(f, dt)                 time_integr_mod.f90:443-569
+    TimeIntegratorMTS_SH_DGV(f, dt)          time_integr_mod.f90:314-364
+    MassCheckRec(f)                          dgvtools_mod.f90:1437-1458
+    maxwelveldist(T, u0, v0, w0, n)          distributions_mod.f90:83-95
+
+Arrays may be numpy arrays (host memory, copied through the library's staging
+buffers) or CUDA torch tensors (used in place).  All arithmetic runs in the
+library's sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_OPT_PROJECT, DGV_OPT_NCHUNKS
+
+PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C}
+
+
+def _ptr(a):
+    """Data pointer of a numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _check_f64(a):
+    dt = getattr(a, "dtype", None)
+    if isinstance(a, np.ndarray):
+        if dt != np.float64:
+            raise TypeError("arrays must be float64")
+    elif str(dt) != "torch.float64":
+        raise TypeError("tensors must be float64")
+
+
+class DGVSolver:
+    """One uniform velocity grid with its A-arrays on one GPU."""
+
+    def __init__(self, s: int = 3, M: int = 5, L: float = 6.0, *, su=None, sv=None, sw=None,
+                 Mu=None, Mv=None, Mw=None, bounds=None, kappa: float = 1.0, device: int = 0,
+                 precision: str = "f64", rkmts: int = 2):
+        self._lib = _lib.load()
+        su = su or s; sv = sv or s; sw = sw or s
+        Mu = Mu or M; Mv = Mv or M; Mw = Mw or M
+        b = bounds or (-L, L, -L, L, -L, L)
+        self.desc = GridDesc(su, sv, sw, Mu, Mv, Mw, *b, kappa)
+        h = C.c_void_p()
+        rc = self._lib.dgv_ctx_create(C.byref(self.desc), device, C.byref(h))
+        if rc != 0:
+            raise DGVError(rc, "dgv_ctx_create failed (grid or device)")
+        self._h = h
+        N = C.c_int64(); P = C.c_int32(); Nc = C.c_int32(); cc = C.c_int32()
+        self._lib.dgv_grid_info(h, C.byref(N), C.byref(P), C.byref(Nc), C.byref(cc))
+        self.N, self.P, self.Nc, self.ccell = N.value, P.value, Nc.value, cc.value
+        self.nodes_u = np.zeros(self.N); self.nodes_v = np.zeros(self.N)
+        self.nodes_w = np.zeros(self.N); self.nodes_gwts = np.zeros(self.N)
+        self._lib.dgv_nodes(h, _ptr(self.nodes_u), _ptr(self.nodes_v), _ptr(self.nodes_w),
+                            _ptr(self.nodes_gwts))
+        self.precision = precision
+        self.rkmts = rkmts
+        self.device = device
+
+    # -- plumbing ------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self._lib.dgv_last_error(self._h)
+            raise DGVError(rc, msg.decode() if msg else "")
+
+    def _prec(self, precision: Optional[str]) -> int:
+        p = precision or self.precision
+        if p not in PRECISIONS:
+            raise ValueError(f"precision must be one of {list(PRECISIONS)}")
+        return PRECISIONS[p]
+
+    @staticmethod
+    def _like(f):
+        if isinstance(f, np.ndarray):
+            return np.zeros_like(f, dtype=np.float64)
+        import torch
+        return torch.zeros_like(f, dtype=torch.float64)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dgv_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._lib.dgv_set_stream(self._h, stream_ptr))
+
+    def set_async(self, flag: bool):
+        self._check(self._lib.dgv_set_async(self._h, int(flag)))
+
+    def set_projection(self, on: bool):
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_PROJECT, int(on)))
+
+    def set_nchunks(self, n: int):
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_NCHUNKS, int(n)))
+
+    # -- A-arrays -------------------------------------------------------------
+    def load_A(self, capphi, A, xi, xi1, one_based: bool = True):
+        """A-arrays in the reference layout (ReadAarraysDGV, readwrite.f90:1066-1118)."""
+        capphi = np.ascontiguousarray(capphi, np.int32)
+        A = np.ascontiguousarray(A, np.float64)
+        xi = np.ascontiguousarray(xi, np.int32)
+        xi1 = np.ascontiguousarray(xi1, np.int32)
+        if capphi.shape != (self.N,):
+            raise ValueError(f"A_capphi must have {self.N} entries")
+        if not (len(A) == len(xi) == len(xi1)):
+            raise ValueError("A, A_xi, A_xi1 lengths differ")
+        self._check(self._lib.dgv_load_A(self._h, len(A), _ptr(capphi), _ptr(A), _ptr(xi),
+                                         _ptr(xi1), int(one_based)))
+
+    ReadAarraysDGV = load_A
+
+    def generate_synthetic_A(self, seed: int = 1, Trad: float = float("inf"), support: int = 1):
+        self._check(self._lib.dgv_generate_A_synthetic(self._h, seed, Trad, support))
+
+    def A_info(self):
+        nr = C.c_int64(); npairs = C.c_int64(); nb = C.c_int64(); rs = C.c_double()
+        self._check(self._lib.dgv_A_info(self._h, C.byref(nr), C.byref(npairs), C.byref(nb),
+                                         C.byref(rs)))
+        return {"records": nr.value, "pairs": npairs.value, "blocks": nb.value,
+                "record_shifts": rs.value}
+
+    def export_A(self):
+        """Loaded A-arrays back in the reference layout (0-based indices)."""
+        n = C.c_int64()
+        self._check(self._lib.dgv_export_A(self._h, C.byref(n), None, None, None, None))
+        capphi = np.zeros(self.N, np.int32)
+        A = np.zeros(n.value); xi = np.zeros(n.value, np.int32); xi1 = np.zeros(n.value, np.int32)
+        self._check(self._lib.dgv_export_A(self._h, C.byref(n), _ptr(capphi), _ptr(A), _ptr(xi),
+                                           _ptr(xi1)))
+        return capphi, A, xi, xi1
+
+    # -- collision operator ---------------------------------------------------
+    def EvalCollisionPeriodicAPlus_DGV(self, f, fc=None, precision=None):
+        _check_f64(f)
+        nb = int(np.prod(f.shape)) // self.N
+        if nb * self.N != int(np.prod(f.shape)):
+            raise ValueError(f"f must hold a multiple of {self.N} values")
+        fc = self._like(f) if fc is None else fc
+        self._check(self._lib.dgv_collide_batched(self._h, nb, _ptr(f), _ptr(fc), self._prec(precision)))
+        return fc
+
+    collide = EvalCollisionPeriodicAPlus_DGV
+
+    def EvalCollisionPeriodicMixedTermsA_DGV(self, f, fm, fc=None):
+        """2/w sum A (fm(xi) f(xi1) + f(xi) fm(xi1)): the JVP of Q at fm along f."""
+        _check_f64(f); _check_f64(fm)
+        fc = self._like(f) if fc is None else fc
+        self._check(self._lib.dgv_jvp(self._h, _ptr(fm), _ptr(f), _ptr(fc), DGV_PREC_F64))
+        return fc
+
+    def jvp(self, f, df, out=None):
+        return self.EvalCollisionPeriodicMixedTermsA_DGV(df, f, out)
+
+    def vjp(self, f, v, out=None):
+        _check_f64(f); _check_f64(v)
+        out = self._like(f) if out is None else out
+        self._check(self._lib.dgv_vjp(self._h, _ptr(f), _ptr(v), _ptr(out), DGV_PREC_F64))
+        return out
+
+    def PrepareFMA_DGV(self, fm):
+        _check_f64(fm)
+        self._check(self._lib.dgv_prepare_linear(self._h, _ptr(fm)))
+
+    def EvalCollisionLinear(self, f, fc=None):
+        _check_f64(f)
+        fc = self._like(f) if fc is None else fc
+        self._check(self._lib.dgv_apply_linear(self._h, _ptr(f), _ptr(fc), DGV_PREC_F64))
+        return fc
+
+    def SpatialOperSH_DGV(self, f, dt, fcol=None, precision=None):
+        _check_f64(f)
+        fcol = self._like(f) if fcol is None else fcol
+        self._check(self._lib.dgv_spatial_oper(self._h, _ptr(f), _ptr(fcol), dt, self._prec(precision)))
+        return fcol
+
+    def project(self, q):
+        nb = int(np.prod(q.shape)) // self.N
+        self._check(self._lib.dgv_project(self._h, _ptr(q), nb))
+        return q
+
+    # -- time integration ----------------------------------------------------
+    def TimeIntegratorORK_SH_DGV(self, f, dt, frhs1=None, order=None, precision=None):
+        """One RK step in place on f; returns frhs1 (first-stage right side / dt)."""
+        _check_f64(f)
+        frhs1 = self._like(f) if frhs1 is None else frhs1
+        self._check(self._lib.dgv_step_rk(self._h, _ptr(f), _ptr(frhs1), dt, order or self.rkmts,
+                                          self._prec(precision)))
+        return frhs1
+
+    def PrepareMTS_SH_DGV(self, f, dt, order=None, precision=None):
+        _check_f64(f)
+        self._check(self._lib.dgv_prepare_ab(self._h, _ptr(f), dt, order or self.rkmts,
+                                             self._prec(precision)))
+
+    def TimeIntegratorMTS_SH_DGV(self, f, dt, precision=None):
+        _check_f64(f)
+        self._check(self._lib.dgv_step_ab(self._h, _ptr(f), dt, self._prec(precision)))
+
+    # -- moments and equilibrium ----------------------------------------------
+    def MassCheckRec(self, f):
+        _check_f64(f)
+        out = np.zeros(5)
+        self._check(self._lib.dgv_moments(self._h, _ptr(f), _ptr(out)))
+        return tuple(out)
+
+    def maxwelveldist(self, T, u0, v0, w0, n, out=None):
+        out = np.zeros(self.N) if out is None else out
+        self._check(self._lib.dgv_maxwellian(self._h, T, u0, v0, w0, n, _ptr(out)))
+        return out

@@ -1,0 +1,163 @@
+/*
+ * dgv_b200.h -- C-ABI of the B200 collision library (libdgv_b200.so).
+ *
+ * Drop-in boundary for the hot path of the DG-velocity Boltzmann solver: the
+ * direct evaluation of the collision integral Q(f,f) and the Runge-Kutta /
+ * Adams-Bashforth stepping that calls it.  Every entry point is `extern "C"`,
+ * takes plain pointers and sizes, returns an int status (never aborts) and is
+ * bind(C)-compatible for a Fortran ISO_C_BINDING interface.  Each declaration
+ * names the reference routine (file:line) it replaces.
+ *
+ * Conventions
+ *   - A context (dgv_ctx) owns one uniform velocity grid, the device copy of
+ *     the collision-information A-arrays and all device work buffers.  It is
+ *     not thread-safe; use one context per host thread.
+ *   - Node arrays (f, q, ...) have N = Mu*Mv*Mw*su*sv*sw entries in the
+ *     reference's node order: cell-major (u outer, v, w inner), then the local
+ *     node (ui, vi, wi) with wi fastest (miscset.f90:882-937, 1112-1183).
+ *   - Array pointers may be host memory (copied through device staging
+ *     buffers inside the call) or device memory (used in place); the library
+ *     asks the CUDA runtime which.  With host pointers every call is
+ *     synchronous; with device pointers the work is ordered on the context's
+ *     stream and the call returns after it completes, unless dgv_set_async(1).
+ *   - Node indices passed in (A_xi, A_xi1) are 1-based when one_based != 0,
+ *     as the reference stores them.
+ */
+#ifndef DGV_B200_H
+#define DGV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DGV_OK 0
+#define DGV_EINVAL 1   /* bad size, layout or argument                       */
+#define DGV_ERANGE 2   /* an index points outside the grid                    */
+#define DGV_ECUDA 3    /* a CUDA runtime call failed                          */
+#define DGV_ETIMEOUT 4 /* a bounded device wait gave up                       */
+#define DGV_ENOMEM 5   /* device or host allocation failed                    */
+#define DGV_ESTATE 6   /* call out of order (e.g. no A-arrays loaded yet)     */
+#define DGV_EUNSUP 7   /* configuration this build does not support           */
+
+/* arithmetic of the collision kernel */
+#define DGV_PREC_F64 0  /* plain FP64 gather-multiply-accumulate               */
+#define DGV_PREC_F32C 1 /* FP32 products, compensated (two-sum) accumulation   */
+
+/* options for dgv_set_option */
+#define DGV_OPT_PROJECT 1  /* 1: apply the FP64 conservation projection to Q  */
+#define DGV_OPT_NCHUNKS 2  /* work chunks per VDF (0 = autotune)             */
+
+typedef struct dgv_ctx dgv_ctx;
+
+/* Uniform velocity grid (SetDGVblzmmesh + Set3DCellsR_DGVblzm + SetNodesDGV,
+ * miscset.f90:210-431, 544-597, 1112-1183) and the dimensionless collision
+ * scale kappa = (mol_diam/L_inf)^2 * N_inf (spat_oper_mod.f90:65). */
+typedef struct {
+    int32_t su, sv, sw;  /* Gauss-Legendre nodes per cell per axis */
+    int32_t Mu, Mv, Mw;  /* cells per axis                        */
+    double u_L, u_R, v_L, v_R, w_L, w_R;
+    double kappa;
+} dgv_grid_desc;
+
+/* -- context ------------------------------------------------------------ */
+/* Builds the grid, nodes, weights and the canonical cell (the cell holding
+ * v = 0, FindCellContainsPoint_DGV dgvtools_mod.f90:1175-1247) on `device`.
+ * Replaces the setup sequence of DGVblzmPL.f90:75-105. */
+int dgv_ctx_create(const dgv_grid_desc *desc, int device, dgv_ctx **out);
+int dgv_ctx_destroy(dgv_ctx *ctx);
+/* message of the last failing call on this context ("" if none) */
+const char *dgv_last_error(const dgv_ctx *ctx);
+/* run on a caller-owned cudaStream_t (NULL = the context's own stream) */
+int dgv_set_stream(dgv_ctx *ctx, void *stream);
+/* 1: device-pointer calls return without synchronising the stream */
+int dgv_set_async(dgv_ctx *ctx, int async_flag);
+int dgv_set_option(dgv_ctx *ctx, int option, int64_t value);
+/* N, P = su*sv*sw, number of cells, canonical cell (0-based) */
+int dgv_grid_info(const dgv_ctx *ctx, int64_t *N, int32_t *P, int32_t *Nc, int32_t *ccell);
+/* host copies of nodes_u/_v/_w/_gwts (miscset.f90:1112-1183); any may be NULL */
+int dgv_nodes(const dgv_ctx *ctx, double *u, double *v, double *w, double *gwts);
+
+/* -- A-arrays ------------------------------------------------------------- */
+/* Uploads A-arrays in the reference layout (commvar.f90:157-167, as read by
+ * ReadAarraysDGV readwrite.f90:1066-1118): capphi[N] records per node,
+ * records of node k contiguous in node order; A[nnz], A_xi[nnz], A_xi1[nnz].
+ * Only the records of canonical-cell nodes are used, as in
+ * EvalCollisionPeriodicAPlus_DGV (collision_mod.f90:186-188).  Converts them
+ * once to the device pair layout; replaces ReadAarrays* + the A part of
+ * SetCellsUGINdsSftArrs (miscset.f90:1202-1311). */
+int dgv_load_A(dgv_ctx *ctx, int64_t nnz, const int32_t *capphi, const double *A,
+               const int32_t *A_xi, const int32_t *A_xi1, int one_based);
+/* Generates synthetic A-arrays on the device with the reference's record
+ * structure: every pair xi<xi1 that passes the SetA_DGV prefilter
+ * (dgvtools_mod.f90:527, cutoff Trad) and, for support_mode 1, whose
+ * collision sphere meets the canonical cell, one record per canonical basis
+ * function with value w_xi*w_xi1*|g|/8*u, u = splitmix64 hash of
+ * (seed, p, xi, xi1) in [-1,1).  No reference counterpart: a seeded stand-in
+ * for A-arrays that take hours to precompute. */
+int dgv_generate_A_synthetic(dgv_ctx *ctx, uint64_t seed, double Trad, int support_mode);
+/* counts of the loaded A-arrays: records, distinct (xi,xi1) pairs, cell-pair
+ * blocks, and record-shift visits per Q evaluation */
+int dgv_A_info(const dgv_ctx *ctx, int64_t *nrecords, int64_t *npairs, int64_t *nblocks,
+               double *record_shifts);
+/* Copies the loaded A-arrays back in the reference layout, 0-based, records
+ * of each canonical basis function grouped by cell pair; nnz_out receives the
+ * count.  Pass NULL arrays to query the size. */
+int dgv_export_A(const dgv_ctx *ctx, int64_t *nnz_out, int32_t *capphi, double *A,
+                 int32_t *A_xi, int32_t *A_xi1);
+
+/* -- collision operator --------------------------------------------------- */
+/* q = Q(f,f) (EvalCollisionPeriodicAPlus_DGV, collision_mod.f90:143-229);
+ * n must equal N. */
+int dgv_collide(dgv_ctx *ctx, const double *f, double *q, int64_t n, int precision);
+/* nb VDFs stored contiguously, f[nb][N] -> q[nb][N] */
+int dgv_collide_batched(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int precision);
+/* fcol = kappa*dt*Q(f,f) (SpatialOperSH_DGV, spat_oper_mod.f90:28-68, run_mode 0) */
+int dgv_spatial_oper(dgv_ctx *ctx, const double *f, double *fcol, double dt, int precision);
+
+/* -- time integration ------------------------------------------------------ */
+/* One optimal Runge-Kutta step of order 1..5 in place on f
+ * (TimeIntegratorORK_SH_DGV, time_integr_mod.f90:26-152).  frhs1 (may be NULL)
+ * receives the first-stage right side divided by dt, as the reference leaves
+ * it in commvar's frhs1. */
+int dgv_step_rk(dgv_ctx *ctx, double *f, double *frhs1, double dt, int order, int precision);
+/* Adams-Bashforth start-up: order-1 RK steps of that order, filling the
+ * right-side history kept in the context (PrepareMTS_SH_DGV, time_integr_mod.f90:443-569). */
+int dgv_prepare_ab(dgv_ctx *ctx, double *f, double dt, int order, int precision);
+/* One Adams-Bashforth step of the order given to dgv_prepare_ab
+ * (TimeIntegratorMTS_SH_DGV, time_integr_mod.f90:314-364). */
+int dgv_step_ab(dgv_ctx *ctx, double *f, double dt, int precision);
+
+/* -- moments, equilibrium, conservation ----------------------------------- */
+/* out = n, ubar, vbar, wbar, T (MassCheckRec, dgvtools_mod.f90:1437-1458) */
+int dgv_moments(dgv_ctx *ctx, const double *f, double out[5]);
+/* f = n exp(-|v-u0|^2/T)/(pi T)^{3/2} at every node (maxwelveldist,
+ * distributions_mod.f90:83-95) */
+int dgv_maxwellian(dgv_ctx *ctx, double T, double u0, double v0, double w0, double n,
+                   double *f);
+/* In place, FP64: removes from q its components along the collision
+ * invariants 1,u,v,w,|v|^2 in the quadrature inner product, so that the
+ * moments the reference monitors (dgvtools_mod.f90:1680-1691) vanish. */
+int dgv_project(dgv_ctx *ctx, double *q, int32_t nb);
+
+/* -- derivatives ----------------------------------------------------------- */
+/* q = 2/w * sum A (f(xi) df(xi1) + df(xi) f(xi1)): the Jacobian-vector product
+ * of Q at f (EvalCollisionPeriodicMixedTermsA_DGV, collision_mod.f90:244-332). */
+int dgv_jvp(dgv_ctx *ctx, const double *f, const double *df, double *q, int precision);
+/* g = J(f)^T v: the vector-Jacobian product of Q at f; g_k = sum_i v_i dQ_i/df_k.
+ * Adjoint of collision_mod.f90:213-216; equals 2*fmA*v at a Maxwellian
+ * (collision_mod.f90:448-449, 357). */
+int dgv_vjp(dgv_ctx *ctx, const double *f, const double *v, double *g, int precision);
+/* Stores the linearisation point fm (PrepareFMA_DGV, collision_mod.f90:377-464).
+ * The dense N x N fmA is not materialised; dgv_apply_linear is matrix-free. */
+int dgv_prepare_linear(dgv_ctx *ctx, const double *fm);
+/* q = 2*MATMUL(df, fmA) at the stored fm (EvalCollisionLinear,
+ * collision_mod.f90:346-359) */
+int dgv_apply_linear(dgv_ctx *ctx, const double *df, double *q, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGV_B200_H */
