@@ -24,7 +24,7 @@ EXPORTS = [
     "dgv_set_option", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_spatial_oper",
     "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
-    "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear",
+    "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
 ]
 
 
@@ -81,6 +81,7 @@ def load() -> C.CDLL:
         "dgv_vjp": [vp, vp, vp, vp, C.c_int],
         "dgv_prepare_linear": [vp, vp],
         "dgv_apply_linear": [vp, vp, vp, C.c_int],
+        "dgv_collide_f64_noalloc": [vp, vp, vp, i32, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

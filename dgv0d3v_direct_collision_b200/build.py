@@ -28,6 +28,7 @@ SOURCES = [
     ("api.cu", []),
     ("collide.cu", []),
     ("adjoint.cu", []),
+    ("noalloc.cu", []),
     ("synth.cu", ["-fmad=false"]),
     ("stepping.cu", ["-fmad=false"]),
 ]

@@ -116,6 +116,20 @@ int dgv_collide(dgv_ctx *ctx, const double *f, double *q, int64_t n, int precisi
 int dgv_collide_batched(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int precision);
 /* fcol = kappa*dt*Q(f,f) (SpatialOperSH_DGV, spat_oper_mod.f90:28-68, run_mode 0) */
 int dgv_spatial_oper(dgv_ctx *ctx, const double *f, double *fcol, double dt, int precision);
+/* No counterpart in the reference.  q = Q(f,f) in FP64, as dgv_collide_batched,
+ * for callers that cannot allocate device memory once they are running -- a
+ * driver that gives all free memory to its own pool allocator at start-up, or
+ * a process held to a fixed memory budget on a shared GPU, where a cudaMalloc
+ * in the time loop would fail or stall the device.  This call allocates
+ * nothing: f and q are caller-owned device arrays [nb][N], and the kernel's
+ * partial sums go to a static 32 MiB device array that every GPU loading the
+ * library holds until the process exits.  Limit: nb*N <= 4194304 (2^22)
+ * doubles, else DGV_EINVAL.  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All calls
+ * share the array and leave their partial sums in it: calls that overlap on
+ * the GPU (other streams or host threads) race, so serialise them.  No
+ * conservation projection.  stream NULL = the context's stream. */
+int dgv_collide_f64_noalloc(dgv_ctx *ctx, const double *f, double *q, int32_t nb, void *stream);
 
 /* -- time integration ------------------------------------------------------ */
 /* One optimal Runge-Kutta step of order 1..5 in place on f
