@@ -305,8 +305,36 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line))
 
 
+def run_profile_case(case: str):
+    """Small case for profiler captures: one VDF on the 21^3 grid (s=3, M=7,
+    [-6,6]^3; A rows ~5.6 GB in total), fixed chunk count (no tuning
+    launches): one warm-up evaluation, then one evaluation to capture."""
+    import torch
+
+    import dgv0d3v_direct_collision_b200 as dgv
+    prec = case.split("_")[0]
+    s = dgv.DGVSolver(3, 7, 6.0)
+    s.generate_synthetic_A(seed=SEED_A, support=1)
+    s.set_nchunks(296)
+    fb = mixture_batch(s.nodes_u, s.nodes_v, s.nodes_w, s.nodes_gwts, 1, 3)
+    f = torch.tensor(fb[0], dtype=torch.float64, device="cuda")
+    q = torch.empty_like(f)
+    times = []
+    for _ in range(2):
+        t = time.perf_counter()
+        if prec == "vjp":
+            s.vjp(f, f, q)
+        else:
+            s.EvalCollisionPeriodicAPlus_DGV(f, q, precision=prec)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    print(json.dumps({"profile_case": case, "wall_s": times, "A": s.A_info()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21"], default=None,
+                    help="small single-VDF case for profiler captures (no JSON bench line)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -316,6 +344,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile_case:
+        run_profile_case(args.profile_case)
+        return
     if args.impl == "reference":
         # the CPU reference runs on rank 0 only; other ranks exit without work
         world = int(os.environ.get("WORLD_SIZE", "1"))

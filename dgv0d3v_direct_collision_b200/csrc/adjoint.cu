@@ -8,12 +8,14 @@
 // Same traversal as the forward kernel: a thread owns an output cell D and
 // keeps its P cotangent weights c_(D,p) in registers; for every pair it forms
 // vA = sum_p A_p c_p (P multiply-adds, the forward's cost) and scatters
-// vA*f(b) to g(a) and vA*f(a) to g(b) with FP64 atomic adds.
+// vA*f(b) to g(a) and vA*f(a) to g(b) with FP64 atomic adds (so the summation
+// order, and the last bits of g, vary from run to run).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
 #include "dgv_internal.h"
+#include "pipeline.cuh"
 
 namespace dgv {
 
@@ -23,24 +25,46 @@ struct VjpArgs {
     const BlockInfo *blk;
     const char *rows;
     const int *bounds;
+    int *err;
     long long N;
-    int Nc, Mv, Mw, dcta, rowb;
+    int Nc, Mv, Mw, dcta, rowb, nst, sp, off_f, off_hdr, off_bar;
 };
 
+// Same shared-memory row pipeline as the forward kernel (pipeline.cuh).
 template <int PV>
-__global__ void __launch_bounds__(384, 1) k_vjp_scatter(VjpArgs a)
+__global__ void __launch_bounds__(416, 1) k_vjp_pipe(VjpArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *f_s = reinterpret_cast<double *>(smem_raw);
-    const int chunk = blockIdx.x, slice = blockIdx.y;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const size_t stage_bytes = (size_t)a.sp * a.rowb;
+    unsigned char *stages = smem;
+    double *f_s = reinterpret_cast<double *>(smem + a.off_f);
+    StageHdr *hdr = reinterpret_cast<StageHdr *>(smem + a.off_hdr);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + a.off_bar);
+    uint64_t *empty = full + a.nst;
+    const int slice = blockIdx.y, chunk = blockIdx.z;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < a.nst; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], a.dcta / 32);
+        }
+        fence_mbar_init();
+    }
     for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
         int cell = (int)(i / PV), l = (int)(i - (long long)cell * PV);
         f_s[l * a.Nc + cell] = __ldg(a.f + i);
     }
     __syncthreads();
-    constexpr int RD = ((1 + PV) + 1) / 2 * 2;
-    const int D = slice * a.dcta + threadIdx.x;
-    const bool inD = (int)threadIdx.x < a.dcta && D < a.Nc;
+    const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
+    const int d0 = slice * a.dcta, d1 = min(a.Nc, d0 + a.dcta);
+    if (threadIdx.x < 32) {  // producer: lane 0 of warp 0
+        if (threadIdx.x == 0)
+            produce_rows(a.blk, b0, b1, a.Mv, a.Mw, d0, d1, a.rows, a.rowb, stages, a.sp, a.nst, hdr, full, empty,
+                         a.err);
+        return;
+    }
+    const int tc = threadIdx.x - 32, lane = threadIdx.x & 31;
+    const int D = d0 + tc;
+    const bool inD = tc < a.dcta && D < a.Nc;
     const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
     double cw[PV];
 #pragma unroll
@@ -48,34 +72,46 @@ __global__ void __launch_bounds__(384, 1) k_vjp_scatter(VjpArgs a)
         long long i = (long long)D * PV + j;
         cw[j] = inD ? 2.0 * a.v[i] / a.w[i] : 0.0;
     }
-    const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
-    for (int b = b0; b < b1; ++b) {
-        const BlockInfo bi = a.blk[b];
-        const bool valid = inD && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
-                           Dw >= bi.lo[2] && Dw <= bi.hi[2];
-        if (!__any_sync(0xffffffffu, valid)) continue;
-        const double2 *row = reinterpret_cast<const double2 *>(a.rows + (size_t)bi.start * a.rowb);
-        for (int k = 0; k < bi.count; ++k, row += RD / 2) {
-            double rv[RD];
+    constexpr int RD = ((1 + PV) + 1) / 2 * 2;
+    int cur = -1;
+    bool valid = false;
+    for (int it = 0;; it++) {
+        const int s = it % a.nst;
+        if (!mbar_wait(&full[s], (it / a.nst) & 1, a.err)) break;
+        const StageHdr h = hdr[s];
+        if (h.block < 0) break;
+        if (h.block != cur) {
+            cur = h.block;
+            const BlockInfo bi = a.blk[cur];
+            valid = inD && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] && Dw >= bi.lo[2] &&
+                    Dw <= bi.hi[2];
+        }
+        if (__any_sync(0xffffffffu, valid) && valid) {
+            const unsigned char *st = stages + s * stage_bytes;
+#pragma unroll 2
+            for (int k = 0; k < h.n; k++) {
+                const double2 *row = reinterpret_cast<const double2 *>(st + (size_t)k * a.rowb);
+                double rv[RD];
 #pragma unroll
-            for (int t = 0; t < RD / 2; t++) {
-                double2 x = __ldg(row + t);
-                rv[2 * t] = x.x;
-                rv[2 * t + 1] = x.y;
-            }
-            if (valid) {
-                long long o = __double_as_longlong(rv[0]);
-                int q1 = (int)(unsigned)(o & 0xffffffffLL) + D, q2 = (int)(o >> 32) + D;
+                for (int t = 0; t < RD / 2; t++) {
+                    double2 x = row[t];
+                    rv[2 * t] = x.x;
+                    rv[2 * t + 1] = x.y;
+                }
+                const long long o = __double_as_longlong(rv[0]);
+                const int q1 = (int)(unsigned)(o & 0xffffffffLL) + D, q2 = (int)(o >> 32) + D;
                 double vA = 0.0;
 #pragma unroll
                 for (int j = 0; j < PV; j++) vA = fma(rv[1 + j], cw[j], vA);
-                int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
-                long long i1 = (long long)(q1 - l1 * a.Nc) * PV + l1;
-                long long i2 = (long long)(q2 - l2 * a.Nc) * PV + l2;
+                const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
+                const long long i1 = (long long)(q1 - l1 * a.Nc) * PV + l1;
+                const long long i2 = (long long)(q2 - l2 * a.Nc) * PV + l2;
                 atomicAdd(a.g + i1, vA * f_s[q2]);
                 atomicAdd(a.g + i2, vA * f_s[q1]);
             }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
     }
 }
 
@@ -86,31 +122,43 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     (void)precision;
     if (!c->lay.blk) return set_err(c, DGV_ESTATE, "vjp: no A-arrays loaded");
     const Grid &g = c->grid;
+    const Layout &L = c->lay;
     VjpFn fn = nullptr;
     switch (g.P) {
-    case 1: fn = k_vjp_scatter<1>; break;
-    case 8: fn = k_vjp_scatter<8>; break;
-    case 27: fn = k_vjp_scatter<27>; break;
+    case 1: fn = k_vjp_pipe<1>; break;
+    case 8: fn = k_vjp_pipe<8>; break;
+    case 27: fn = k_vjp_pipe<27>; break;
     default: return set_err(c, DGV_EUNSUP, "vjp: this build supports 1, 8 or 27 nodes per cell");
     }
-    int nc32 = (g.Nc + 31) / 32 * 32;
-    int dcta = std::min(nc32, 384), slices = (g.Nc + dcta - 1) / dcta;
-    size_t smem = (size_t)g.N * sizeof(double);
     int maxsm = 0, nsm = 148;
     DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     DGV_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    if (smem > (size_t)maxsm) return set_err(c, DGV_EUNSUP, "vjp: f does not fit in shared memory for this grid");
+    const int nc32 = (g.Nc + 31) / 32 * 32;
+    const int dcta = std::min(nc32, 384), slices = (g.Nc + dcta - 1) / dcta;
+    const int rowb = L.RD64 * 8, nst = 6;
+    const size_t fbytes = (size_t)g.N * sizeof(double);
+    const size_t tail = 16 + nst * sizeof(StageHdr) + 2 * nst * sizeof(uint64_t) + 16;
+    if (fbytes + tail + (size_t)nst * 4 * rowb > (size_t)maxsm)
+        return set_err(c, DGV_EUNSUP, "vjp: f does not fit in shared memory for this grid");
+    const size_t ring = std::min<size_t>(64 * 1024, (size_t)maxsm - fbytes - tail);
+    const int sp = (int)std::min<size_t>(256, ring / ((size_t)nst * rowb));
+    VjpArgs a;
+    a.off_f = nst * sp * rowb;
+    a.off_hdr = (int)((a.off_f + fbytes + 15) / 16 * 16);
+    a.off_bar = a.off_hdr + nst * (int)sizeof(StageHdr);
+    const size_t smem = (size_t)a.off_bar + 2 * nst * sizeof(uint64_t);
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int nchunks = std::max(1, std::min<int>(2 * nsm / slices, (int)std::max<long long>(1, c->lay.nblocks)));
+    int nchunks = std::max(1, std::min<int>(2 * nsm / slices, (int)std::max<long long>(1, L.nblocks)));
     int *d_bounds = nullptr;
     int rc = get_chunks(c, nchunks, &d_bounds);
     if (rc) return rc;
+    rc = ensure_errflag(c);
+    if (rc) return rc;
     DGV_CUDA(c, cudaMemsetAsync(d_g, 0, sizeof(double) * (size_t)g.N, c->stream));
-    VjpArgs a;
-    a.f = d_f; a.v = d_v; a.w = c->d_nwt; a.g = d_g; a.blk = c->lay.blk; a.rows = (const char *)c->lay.rows64;
-    a.bounds = d_bounds; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.dcta = dcta;
-    a.rowb = c->lay.RD64 * 8;
-    fn<<<dim3(nchunks, slices, 1), dcta, smem, c->stream>>>(a);
+    a.f = d_f; a.v = d_v; a.w = c->d_nwt; a.g = d_g; a.blk = L.blk; a.rows = (const char *)L.rows64;
+    a.bounds = d_bounds; a.err = c->d_err; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.dcta = dcta;
+    a.rowb = rowb; a.nst = nst; a.sp = sp;
+    fn<<<dim3(1, slices, nchunks), 32 + dcta, smem, c->stream>>>(a);
     DGV_CUDA(c, cudaGetLastError());
     return DGV_OK;
 }

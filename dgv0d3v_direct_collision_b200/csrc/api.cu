@@ -44,6 +44,26 @@ int ensure_buffer(Ctx *c, double **p, size_t *have, size_t need_bytes)
     return DGV_OK;
 }
 
+int ensure_errflag(Ctx *c)
+{
+    if (c->d_err) return DGV_OK;
+    DGV_CUDA(c, cudaHostAlloc((void **)&c->h_err, sizeof(int), cudaHostAllocMapped));
+    *(volatile int *)c->h_err = 0;
+    DGV_CUDA(c, cudaHostGetDevicePointer((void **)&c->d_err, c->h_err, 0));
+    return DGV_OK;
+}
+
+// After the stream has synchronised: report (and clear) a bounded device wait
+// that gave up.
+int check_errflag(Ctx *c)
+{
+    if (c->h_err && *(volatile int *)c->h_err) {
+        *(volatile int *)c->h_err = 0;
+        return set_err(c, DGV_ETIMEOUT, "a bounded device wait in a collision kernel gave up; results discarded");
+    }
+    return DGV_OK;
+}
+
 static bool is_device_ptr(const void *p)
 {
     cudaPointerAttributes at;
@@ -98,6 +118,7 @@ static void destroy_ctx(Ctx *c)
         if (p) cudaFree(p);
     for (double *p : c->d_hist)
         if (p) cudaFree(p);
+    if (c->h_err) cudaFreeHost(c->h_err);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
 
@@ -138,7 +159,10 @@ static int out_ptr(Ctx *c, double *p, size_t n, double **d, bool *host)
 static int finish(Ctx *c, double *host_dst, const double *d_src, size_t n, bool host)
 {
     if (host) DGV_CUDA(c, cudaMemcpyAsync(host_dst, d_src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (host || !c->async) DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (host || !c->async) {
+        DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+        return check_errflag(c);
+    }
     return DGV_OK;
 }
 
@@ -193,6 +217,11 @@ int dgv_ctx_create(const dgv_grid_desc *desc, int device, dgv_ctx **out)
             delete h;
             return DGV_ENOMEM;
         }
+    }
+    if (ensure_errflag(c)) {
+        destroy_ctx(c);
+        delete h;
+        return DGV_ECUDA;
     }
     *out = h;
     return DGV_OK;
@@ -353,7 +382,10 @@ int dgv_step_rk(dgv_ctx *ctx, double *f, double *frhs1, double dt, int order, in
     TRY(rk_step_device(c, df, dr, dt, order, precision));
     if (!fdev) DGV_CUDA(c, cudaMemcpyAsync(f, df, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (rhost) DGV_CUDA(c, cudaMemcpyAsync(frhs1, dr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (!fdev || rhost || !c->async) DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!fdev || rhost || !c->async) {
+        DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+        return check_errflag(c);
+    }
     return DGV_OK;
 }
 
@@ -372,7 +404,10 @@ static int ab_common(dgv_ctx *ctx, double *f, double dt, int order, int precisio
     }
     TRY(prepare ? ab_prepare_device(c, df, dt, order, precision) : ab_step_device(c, df, dt, precision));
     if (!fdev) DGV_CUDA(c, cudaMemcpyAsync(f, df, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (!fdev || !c->async) DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!fdev || !c->async) {
+        DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+        return check_errflag(c);
+    }
     return DGV_OK;
 }
 

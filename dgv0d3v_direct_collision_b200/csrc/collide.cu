@@ -24,10 +24,14 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "dgv_internal.h"
+#include "pipeline.cuh"
 
 namespace dgv {
+
+enum CollideMode { MODE_F64 = 0, MODE_F32C = 1, MODE_BILINEAR = 2 };
 
 struct CollideArgs {
     const double *f;        // [nvdf][N]
@@ -36,67 +40,14 @@ struct CollideArgs {
     const BlockInfo *blk;
     const char *rows;
     const int *bounds;      // [nchunks+1]
+    int *err;               // raised by a bounded wait that gave up
     long long N;
     int Nc, Mv, Mw, nchunks, dcta, rowb;
+    int nst, sp;            // pipeline stages, pairs per stage
+    int off_f, off_hdr, off_bar;  // shared-memory layout (bytes)
 };
 
-// -------------------------------------------------------------------------
-// FP64
-template <int PV>
-__global__ void __launch_bounds__(384, 1) k_collide_f64(CollideArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *f_s = reinterpret_cast<double *>(smem_raw);
-    const int vdf = blockIdx.x, slice = blockIdx.y, chunk = blockIdx.z;
-    const double *f = a.f + (size_t)vdf * a.N;
-    for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
-        int cell = (int)(i / PV), l = (int)(i - (long long)cell * PV);
-        f_s[l * a.Nc + cell] = __ldg(f + i);
-    }
-    __syncthreads();
-    constexpr int RD = ((1 + PV) + 1) / 2 * 2;
-    const int D = slice * a.dcta + threadIdx.x;
-    const bool inD = (int)threadIdx.x < a.dcta && D < a.Nc;
-    const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
-    double acc[PV];
-#pragma unroll
-    for (int j = 0; j < PV; j++) acc[j] = 0.0;
-    const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
-    for (int b = b0; b < b1; ++b) {
-        const BlockInfo bi = a.blk[b];
-        const bool valid = inD && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
-                           Dw >= bi.lo[2] && Dw <= bi.hi[2];
-        if (!__any_sync(0xffffffffu, valid)) continue;
-        const double2 *row = reinterpret_cast<const double2 *>(a.rows + (size_t)bi.start * a.rowb);
-        for (int k = 0; k < bi.count; ++k, row += RD / 2) {
-            double rv[RD];
-#pragma unroll
-            for (int t = 0; t < RD / 2; t++) {
-                double2 x = __ldg(row + t);
-                rv[2 * t] = x.x;
-                rv[2 * t + 1] = x.y;
-            }
-            if (valid) {
-                long long o = __double_as_longlong(rv[0]);
-                int o1 = (int)(unsigned)(o & 0xffffffffLL), o2 = (int)(o >> 32);
-                double prod = f_s[o1 + D] * f_s[o2 + D];
-#pragma unroll
-                for (int j = 0; j < PV; j++) acc[j] = fma(rv[1 + j], prod, acc[j]);
-            }
-        }
-    }
-    if (inD) {
-        double *out = a.partial + ((size_t)vdf * a.nchunks + chunk) * PV * a.Nc;
-#pragma unroll
-        for (int j = 0; j < PV; j++) out[(size_t)j * a.Nc + D] = acc[j];
-    }
-}
-
-// -------------------------------------------------------------------------
-// FP32 products with compensated accumulation.  Within a group of at most
-// 16 pairs the P partial sums run in FP32; each group sum is then added to a
-// (sum, correction) pair with Knuth's branch-free two-sum, so the rounding of
-// the long accumulation is carried along instead of lost.
+// Knuth's branch-free two-sum: s + c carries x exactly
 __device__ __forceinline__ void two_sum_acc(float &s, float &c, float x)
 {
     float t = s + x;
@@ -106,121 +57,175 @@ __device__ __forceinline__ void two_sum_acc(float &s, float &c, float x)
     c += err;
 }
 
-template <int PV>
-__global__ void __launch_bounds__(384, 1) k_collide_f32c(CollideArgs a)
+// Shared memory: [NST stages of SP rows][f_s: local-major copy of f][stage
+// headers][full/empty mbarriers].  Warp 0 is the producer (its lane 0 issues
+// the bulk copies); the other warps are consumers, one output cell each.
+//   MODE_F64      acc_p += v_p * f(a) f(b)                       (FP64)
+//   MODE_F32C     FP32 products; groups of <= 16 pairs summed in FP32 and
+//                 added to (sum, correction) with two-sum
+//   MODE_BILINEAR acc_p += v_p * (f(a) g(b) + g(a) f(b)), g gathered from
+//                 global memory (the Jacobian-vector product)
+template <int PV, int MODE>
+__global__ void __maxnreg__(152) k_collide_pipe(CollideArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *f_s = reinterpret_cast<float *>(smem_raw);
+    using T = typename std::conditional<MODE == MODE_F32C, float, double>::type;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const size_t stage_bytes = (size_t)a.sp * a.rowb;
+    unsigned char *stages = smem;
+    T *f_s = reinterpret_cast<T *>(smem + a.off_f);
+    StageHdr *hdr = reinterpret_cast<StageHdr *>(smem + a.off_hdr);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + a.off_bar);
+    uint64_t *empty = full + a.nst;
     const int vdf = blockIdx.x, slice = blockIdx.y, chunk = blockIdx.z;
+    const int nconsumer_warps = a.dcta / 32;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < a.nst; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], nconsumer_warps);
+        }
+        fence_mbar_init();
+    }
     const double *f = a.f + (size_t)vdf * a.N;
     for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
         int cell = (int)(i / PV), l = (int)(i - (long long)cell * PV);
-        f_s[l * a.Nc + cell] = __double2float_rn(__ldg(f + i));
+        f_s[l * a.Nc + cell] = (T)__ldg(f + i);
     }
     __syncthreads();
-    constexpr int RW = ((2 + PV) + 3) / 4 * 4;
-    const int D = slice * a.dcta + threadIdx.x;
-    const bool inD = (int)threadIdx.x < a.dcta && D < a.Nc;
-    const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
-    float s[PV], cmp[PV], part[PV];
-#pragma unroll
-    for (int j = 0; j < PV; j++) { s[j] = 0.f; cmp[j] = 0.f; part[j] = 0.f; }
     const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
-    for (int b = b0; b < b1; ++b) {
-        const BlockInfo bi = a.blk[b];
-        const bool valid = inD && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
-                           Dw >= bi.lo[2] && Dw <= bi.hi[2];
-        if (!__any_sync(0xffffffffu, valid)) continue;
-        const float4 *row = reinterpret_cast<const float4 *>(a.rows + (size_t)bi.start * a.rowb);
-        int n = 0;
-        for (int k = 0; k < bi.count; ++k, row += RW / 4) {
-            float rv[RW];
+    const int d0 = slice * a.dcta, d1 = min(a.Nc, d0 + a.dcta);
+
+    if (threadIdx.x < 32) {  // producer: lane 0 of warp 0
+        if (threadIdx.x == 0)
+            produce_rows(a.blk, b0, b1, a.Mv, a.Mw, d0, d1, a.rows, a.rowb, stages, a.sp, a.nst, hdr, full, empty,
+                         a.err);
+        return;
+    }
+
+    // ---------------- consumers: one output cell D per thread ----------------
+    const int tc = threadIdx.x - 32, lane = threadIdx.x & 31;
+    const int D = d0 + tc;
+    const bool inD = tc < a.dcta && D < a.Nc;
+    const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
+    const double *g = (MODE == MODE_BILINEAR) ? a.f2 + (size_t)vdf * a.N : nullptr;
+    T acc[PV];
+    float cmp[MODE == MODE_F32C ? PV : 1], part[MODE == MODE_F32C ? PV : 1];
 #pragma unroll
-            for (int t = 0; t < RW / 4; t++) {
-                float4 x = __ldg(row + t);
-                rv[4 * t] = x.x; rv[4 * t + 1] = x.y; rv[4 * t + 2] = x.z; rv[4 * t + 3] = x.w;
+    for (int j = 0; j < PV; j++) acc[j] = (T)0;
+    if constexpr (MODE == MODE_F32C) {
+#pragma unroll
+        for (int j = 0; j < PV; j++) { cmp[j] = 0.f; part[j] = 0.f; }
+    }
+    int npend = 0;  // pairs in the open FP32 group
+    int cur = -1;
+    bool valid = false;
+    constexpr int RD = ((1 + PV) + 1) / 2 * 2;  // FP64 row, doubles
+    constexpr int RW = ((2 + PV) + 3) / 4 * 4;  // FP32 row, words
+    for (int it = 0;; it++) {
+        const int s = it % a.nst;
+        if (!mbar_wait(&full[s], (it / a.nst) & 1, a.err)) break;
+        const StageHdr h = hdr[s];
+        if (h.block < 0) break;
+        if (h.block != cur) {
+            if constexpr (MODE == MODE_F32C) {
+                if (valid && npend) {
+#pragma unroll
+                    for (int j = 0; j < PV; j++) { two_sum_acc(acc[j], cmp[j], part[j]); part[j] = 0.f; }
+                    npend = 0;
+                }
             }
-            if (valid) {
-                int o1 = __float_as_int(rv[0]), o2 = __float_as_int(rv[1]);
-                float prod = f_s[o1 + D] * f_s[o2 + D];
+            cur = h.block;
+            const BlockInfo bi = a.blk[cur];
+            valid = inD && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] && Dw >= bi.lo[2] &&
+                    Dw <= bi.hi[2];
+        }
+        if (__any_sync(0xffffffffu, valid) && valid) {
+            const unsigned char *st = stages + s * stage_bytes;
+            // software pipeline over the stage's pairs: the gathers of pair k+1
+            // are issued before the multiply-adds of pair k, so their latency
+            // overlaps arithmetic
+            if constexpr (MODE == MODE_F32C) {
+                const int *ow = reinterpret_cast<const int *>(st);
+                const int rws = a.rowb / 4;
+                float pa = f_s[ow[0] + D], pb = f_s[ow[1] + D];
+                for (int k = 0; k < h.n; k++) {
+                    const float prod = pa * pb;
+                    if (k + 1 < h.n) {
+                        pa = f_s[ow[(k + 1) * rws] + D];
+                        pb = f_s[ow[(k + 1) * rws + 1] + D];
+                    }
+                    const float4 *row = reinterpret_cast<const float4 *>(st + (size_t)k * a.rowb);
+                    float rv[RW];
 #pragma unroll
-                for (int j = 0; j < PV; j++) part[j] = fmaf(rv[2 + j], prod, part[j]);
-                if (++n == 16) {
+                    for (int t = 0; t < RW / 4; t++) {
+                        float4 x = row[t];
+                        rv[4 * t] = x.x; rv[4 * t + 1] = x.y; rv[4 * t + 2] = x.z; rv[4 * t + 3] = x.w;
+                    }
 #pragma unroll
-                    for (int j = 0; j < PV; j++) { two_sum_acc(s[j], cmp[j], part[j]); part[j] = 0.f; }
-                    n = 0;
+                    for (int j = 0; j < PV; j++) part[j] = fmaf(rv[2 + j], prod, part[j]);
+                    if (++npend == 16) {
+#pragma unroll
+                        for (int j = 0; j < PV; j++) { two_sum_acc(acc[j], cmp[j], part[j]); part[j] = 0.f; }
+                        npend = 0;
+                    }
+                }
+            } else {
+                const int *ow = reinterpret_cast<const int *>(st);
+                const int rws = a.rowb / 4;
+                int q1 = ow[0] + D, q2 = ow[1] + D;
+                double pa = f_s[q1], pb = f_s[q2];
+                double ga = 0.0, gb = 0.0;
+                if constexpr (MODE == MODE_BILINEAR) {
+                    const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
+                    ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PV + l1);
+                    gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PV + l2);
+                }
+                for (int k = 0; k < h.n; k++) {
+                    double prod;
+                    if constexpr (MODE == MODE_BILINEAR) prod = pa * gb + ga * pb;
+                    else prod = pa * pb;
+                    if (k + 1 < h.n) {
+                        q1 = ow[(k + 1) * rws] + D;
+                        q2 = ow[(k + 1) * rws + 1] + D;
+                        pa = f_s[q1];
+                        pb = f_s[q2];
+                        if constexpr (MODE == MODE_BILINEAR) {
+                            const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
+                            ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PV + l1);
+                            gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PV + l2);
+                        }
+                    }
+                    // values v[0..P-1] start at byte 8 of the row
+                    const double *row = reinterpret_cast<const double *>(st + (size_t)k * a.rowb);
+                    const double2 *row2 = reinterpret_cast<const double2 *>(row);
+                    double rv[RD];
+#pragma unroll
+                    for (int t = 0; t < RD / 2; t++) {
+                        double2 x = row2[t];
+                        rv[2 * t] = x.x;
+                        rv[2 * t + 1] = x.y;
+                    }
+#pragma unroll
+                    for (int j = 0; j < PV; j++) acc[j] = fma(rv[1 + j], prod, acc[j]);
                 }
             }
         }
-        if (valid && n) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if constexpr (MODE == MODE_F32C) {
+        if (valid && npend) {
 #pragma unroll
-            for (int j = 0; j < PV; j++) { two_sum_acc(s[j], cmp[j], part[j]); part[j] = 0.f; }
+            for (int j = 0; j < PV; j++) { two_sum_acc(acc[j], cmp[j], part[j]); part[j] = 0.f; }
         }
     }
     if (inD) {
         double *out = a.partial + ((size_t)vdf * a.nchunks + chunk) * PV * a.Nc;
 #pragma unroll
-        for (int j = 0; j < PV; j++) out[(size_t)j * a.Nc + D] = (double)s[j] + (double)cmp[j];
-    }
-}
-
-// -------------------------------------------------------------------------
-// Bilinear form for the Jacobian-vector product: prod = f(a) g(b) + g(a) f(b)
-// (collision_mod.f90:290-292).  The second argument is gathered from global
-// memory (L1/L2) so that the shared copy of f still fits at large grids.
-template <int PV>
-__global__ void __launch_bounds__(384, 1) k_bilinear_f64(CollideArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *f_s = reinterpret_cast<double *>(smem_raw);
-    const int vdf = blockIdx.x, slice = blockIdx.y, chunk = blockIdx.z;
-    const double *f = a.f + (size_t)vdf * a.N;
-    const double *g = a.f2 + (size_t)vdf * a.N;
-    for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
-        int cell = (int)(i / PV), l = (int)(i - (long long)cell * PV);
-        f_s[l * a.Nc + cell] = __ldg(f + i);
-    }
-    __syncthreads();
-    constexpr int RD = ((1 + PV) + 1) / 2 * 2;
-    const int D = slice * a.dcta + threadIdx.x;
-    const bool inD = (int)threadIdx.x < a.dcta && D < a.Nc;
-    const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
-    double acc[PV];
-#pragma unroll
-    for (int j = 0; j < PV; j++) acc[j] = 0.0;
-    const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
-    for (int b = b0; b < b1; ++b) {
-        const BlockInfo bi = a.blk[b];
-        const bool valid = inD && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
-                           Dw >= bi.lo[2] && Dw <= bi.hi[2];
-        if (!__any_sync(0xffffffffu, valid)) continue;
-        const double2 *row = reinterpret_cast<const double2 *>(a.rows + (size_t)bi.start * a.rowb);
-        for (int k = 0; k < bi.count; ++k, row += RD / 2) {
-            double rv[RD];
-#pragma unroll
-            for (int t = 0; t < RD / 2; t++) {
-                double2 x = __ldg(row + t);
-                rv[2 * t] = x.x;
-                rv[2 * t + 1] = x.y;
-            }
-            if (valid) {
-                long long o = __double_as_longlong(rv[0]);
-                int o1 = (int)(unsigned)(o & 0xffffffffLL), o2 = (int)(o >> 32);
-                // global node index of the gathered shared-memory word o + D
-                int q1 = o1 + D, q2 = o2 + D;
-                int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
-                long long i1 = (long long)(q1 - l1 * a.Nc) * PV + l1;
-                long long i2 = (long long)(q2 - l2 * a.Nc) * PV + l2;
-                double prod = f_s[q1] * __ldg(g + i2) + __ldg(g + i1) * f_s[q2];
-#pragma unroll
-                for (int j = 0; j < PV; j++) acc[j] = fma(rv[1 + j], prod, acc[j]);
-            }
+        for (int j = 0; j < PV; j++) {
+            double v = (double)acc[j];
+            if constexpr (MODE == MODE_F32C) v += (double)cmp[j];
+            out[(size_t)j * a.Nc + D] = v;
         }
-    }
-    if (inD) {
-        double *out = a.partial + ((size_t)vdf * a.nchunks + chunk) * PV * a.Nc;
-#pragma unroll
-        for (int j = 0; j < PV; j++) out[(size_t)j * a.Nc + D] = acc[j];
     }
 }
 
@@ -246,47 +251,54 @@ __global__ void k_reduce_chunks(const double *partial, const double *w, double *
 // -------------------------------------------------------------------------
 typedef void (*KernelFn)(CollideArgs);
 
-static KernelFn pick_kernel(int P, int precision, bool bilinear)
+static KernelFn pick_kernel(int P, int mode)
 {
-    if (bilinear) {
-        switch (P) {
-        case 1: return k_bilinear_f64<1>;
-        case 8: return k_bilinear_f64<8>;
-        case 27: return k_bilinear_f64<27>;
-        default: return nullptr;
-        }
-    }
-    if (precision == DGV_PREC_F64) {
-        switch (P) {
-        case 1: return k_collide_f64<1>;
-        case 8: return k_collide_f64<8>;
-        case 27: return k_collide_f64<27>;
-        default: return nullptr;
-        }
-    }
+#define DGV_PICK(PV)                                              \
+    case PV:                                                      \
+        if (mode == MODE_F64) return k_collide_pipe<PV, MODE_F64>;  \
+        if (mode == MODE_F32C) return k_collide_pipe<PV, MODE_F32C>; \
+        return k_collide_pipe<PV, MODE_BILINEAR>;
     switch (P) {
-    case 1: return k_collide_f32c<1>;
-    case 8: return k_collide_f32c<8>;
-    case 27: return k_collide_f32c<27>;
+        DGV_PICK(1)
+        DGV_PICK(8)
+        DGV_PICK(27)
     default: return nullptr;
     }
+#undef DGV_PICK
 }
 
 struct LaunchShape {
-    int dcta, slices, threads;
+    int dcta, slices, threads, nst, sp, off_f, off_hdr, off_bar;
     size_t smem;
 };
 
-static LaunchShape shape_for(const Ctx *c, int precision)
+// Pipeline geometry: consumers = one warp per 32 output cells (<= 384), plus
+// the producer warp; the stage ring takes what shared memory the copy of f
+// leaves, up to 64 KiB, in 4-6 stages.
+static int shape_for(Ctx *c, int mode, LaunchShape &s)
 {
     const Grid &g = c->grid;
-    LaunchShape s;
-    int nc32 = (g.Nc + 31) / 32 * 32;
+    const Layout &L = c->lay;
+    int maxsm = 0;
+    DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    const int nc32 = (g.Nc + 31) / 32 * 32;
     s.dcta = std::min(nc32, 384);
     s.slices = (g.Nc + s.dcta - 1) / s.dcta;
-    s.threads = s.dcta;
-    s.smem = (size_t)g.N * (precision == DGV_PREC_F64 ? sizeof(double) : sizeof(float));
-    return s;
+    s.threads = 32 + s.dcta;
+    const int rowb = mode == MODE_F32C ? L.RW32 * 4 : L.RD64 * 8;
+    const size_t fbytes = (size_t)g.N * (mode == MODE_F32C ? sizeof(float) : sizeof(double));
+    const int nst = 6;
+    const size_t tail = 16 + (size_t)nst * sizeof(StageHdr) + 2 * nst * sizeof(uint64_t) + 16;
+    if (fbytes + tail + (size_t)nst * 4 * rowb > (size_t)maxsm)
+        return set_err(c, DGV_EUNSUP, "collide: f of one VDF does not fit in shared memory for this grid");
+    size_t ring = std::min<size_t>(64 * 1024, (size_t)maxsm - fbytes - tail);
+    s.nst = nst;
+    s.sp = (int)std::min<size_t>(256, ring / ((size_t)nst * rowb));
+    s.off_f = s.nst * s.sp * rowb;
+    s.off_hdr = (int)((s.off_f + fbytes + 15) / 16 * 16);
+    s.off_bar = s.off_hdr + s.nst * (int)sizeof(StageHdr);
+    s.smem = (size_t)s.off_bar + 2 * s.nst * sizeof(uint64_t);
+    return DGV_OK;
 }
 
 static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_q, int nvdf, int precision,
@@ -294,29 +306,30 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
-    const bool bilinear = d_f2 != nullptr;
-    KernelFn fn = pick_kernel(g.P, precision, bilinear);
+    const int mode = d_f2 ? MODE_BILINEAR : (precision == DGV_PREC_F64 ? MODE_F64 : MODE_F32C);
+    KernelFn fn = pick_kernel(g.P, mode);
     if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8 or 27 nodes per cell");
-    LaunchShape sh = shape_for(c, bilinear ? DGV_PREC_F64 : precision);
-    int maxsm = 0;
-    DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    if (sh.smem > (size_t)maxsm)
-        return set_err(c, DGV_EUNSUP, "collide: f of one VDF does not fit in shared memory for this grid");
+    LaunchShape sh;
+    int rc = shape_for(c, mode, sh);
+    if (rc) return rc;
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     nchunks = std::max(1, std::min<int>(nchunks, (int)std::max<long long>(1, L.nblocks)));
+    if (nchunks > 65535) return set_err(c, DGV_EINVAL, "collide: at most 65535 chunks");
     int *d_bounds = nullptr;
-    int rc = get_chunks(c, nchunks, &d_bounds);
+    rc = get_chunks(c, nchunks, &d_bounds);
     if (rc) return rc;
     size_t need = (size_t)nvdf * nchunks * g.P * g.Nc * sizeof(double);
     rc = ensure_buffer(c, &c->d_partial, &c->partial_bytes, need);
     if (rc) return rc;
+    rc = ensure_errflag(c);
+    if (rc) return rc;
     CollideArgs a;
-    a.f = d_f; a.f2 = d_f2; a.partial = c->d_partial; a.blk = L.blk;
-    a.rows = (const char *)((precision == DGV_PREC_F64 || bilinear) ? L.rows64 : L.rows32);
-    a.rowb = (precision == DGV_PREC_F64 || bilinear) ? L.RD64 * 8 : L.RW32 * 4;
+    a.f = d_f; a.f2 = d_f2; a.partial = c->d_partial; a.blk = L.blk; a.err = c->d_err;
+    a.rows = (const char *)(mode == MODE_F32C ? L.rows32 : L.rows64);
+    a.rowb = mode == MODE_F32C ? L.RW32 * 4 : L.RD64 * 8;
     a.bounds = d_bounds; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw;
-    a.nchunks = nchunks; a.dcta = sh.dcta;
-    if (nchunks > 65535) return set_err(c, DGV_EINVAL, "collide: at most 65535 chunks");
+    a.nchunks = nchunks; a.dcta = sh.dcta; a.nst = sh.nst; a.sp = sh.sp;
+    a.off_f = sh.off_f; a.off_hdr = sh.off_hdr; a.off_bar = sh.off_bar;
     // VDF fastest: the CTAs resident at one time work on the same chunk of
     // rows for different VDFs, so each row is fetched from HBM once and then
     // served from L2
@@ -336,7 +349,9 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
 {
     if (c->nchunks_opt > 0) return c->nchunks_opt;
     const Grid &g = c->grid;
-    LaunchShape sh = shape_for(c, precision);
+    LaunchShape sh;
+    int rc0 = shape_for(c, d_f2 ? MODE_BILINEAR : (precision == DGV_PREC_F64 ? MODE_F64 : MODE_F32C), sh);
+    if (rc0) return 1;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
     long long units = (long long)nvdf * sh.slices;

@@ -92,6 +92,9 @@ struct Ctx {
     int ab_order = 0;
     // linearisation point
     double *d_fm = nullptr;
+    // error flag raised by a bounded device wait that gave up: pinned host
+    // memory mapped into the device (h_err and d_err alias the same int)
+    int *h_err = nullptr, *d_err = nullptr;
     // autotuned chunk counts keyed by (precision, nvdf bucket)
     std::map<long long, int> tuned;
 };
@@ -108,6 +111,8 @@ int set_err(Ctx *c, int code, const std::string &msg);
 
 int ensure_buffer(Ctx *c, double **p, size_t *have, size_t need_bytes);
 void release_graphs(const Ctx *c);
+int ensure_errflag(Ctx *c);
+int check_errflag(Ctx *c);
 
 // layout construction
 int layout_from_reference(Ctx *c, long long nnz, const int32_t *capphi, const double *A,
