@@ -32,7 +32,7 @@ struct VjpArgs {
 
 // Same shared-memory row pipeline as the forward kernel (pipeline.cuh).
 template <int PV>
-__global__ void __launch_bounds__(416, 1) k_vjp_pipe(VjpArgs a)
+__global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const size_t stage_bytes = (size_t)a.sp * a.rowb;
@@ -133,8 +133,8 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     int maxsm = 0, nsm = 148;
     DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     DGV_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    const int nc32 = (g.Nc + 31) / 32 * 32;
-    const int dcta = std::min(nc32, 384), slices = (g.Nc + dcta - 1) / dcta;
+    const int slices = (g.Nc + 351) / 352;
+    const int dcta = ((g.Nc + slices - 1) / slices + 31) / 32 * 32;
     const int rowb = L.RD64 * 8, nst = 6;
     const size_t fbytes = (size_t)g.N * sizeof(double);
     const size_t tail = 16 + nst * sizeof(StageHdr) + 2 * nst * sizeof(uint64_t) + 16;

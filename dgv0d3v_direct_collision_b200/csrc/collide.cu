@@ -66,7 +66,7 @@ __device__ __forceinline__ void two_sum_acc(float &s, float &c, float x)
 //   MODE_BILINEAR acc_p += v_p * (f(a) g(b) + g(a) f(b)), g gathered from
 //                 global memory (the Jacobian-vector product)
 template <int PV, int MODE>
-__global__ void __maxnreg__(152) k_collide_pipe(CollideArgs a)
+__global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
 {
     using T = typename std::conditional<MODE == MODE_F32C, float, double>::type;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -194,18 +194,16 @@ __global__ void __maxnreg__(152) k_collide_pipe(CollideArgs a)
                             gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PV + l2);
                         }
                     }
-                    // values v[0..P-1] start at byte 8 of the row
-                    const double *row = reinterpret_cast<const double *>(st + (size_t)k * a.rowb);
-                    const double2 *row2 = reinterpret_cast<const double2 *>(row);
-                    double rv[RD];
+                    // values v[0..P-1] start at byte 8 of the row; each 16-byte
+                    // load is consumed at once to keep few values live
+                    const double2 *row2 = reinterpret_cast<const double2 *>(st + (size_t)k * a.rowb);
+                    acc[0] = fma(row2[0].y, prod, acc[0]);
 #pragma unroll
-                    for (int t = 0; t < RD / 2; t++) {
-                        double2 x = row2[t];
-                        rv[2 * t] = x.x;
-                        rv[2 * t + 1] = x.y;
+                    for (int t = 1; t < RD / 2; t++) {
+                        const double2 x = row2[t];
+                        if (2 * t - 1 < PV) acc[2 * t - 1] = fma(x.x, prod, acc[2 * t - 1]);
+                        if (2 * t < PV) acc[2 * t] = fma(x.y, prod, acc[2 * t]);
                     }
-#pragma unroll
-                    for (int j = 0; j < PV; j++) acc[j] = fma(rv[1 + j], prod, acc[j]);
                 }
             }
         }
@@ -281,9 +279,10 @@ static int shape_for(Ctx *c, int mode, LaunchShape &s)
     const Layout &L = c->lay;
     int maxsm = 0;
     DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    const int nc32 = (g.Nc + 31) / 32 * 32;
-    s.dcta = std::min(nc32, 384);
-    s.slices = (g.Nc + s.dcta - 1) / s.dcta;
+    // at most 11 consumer warps + the producer: 12 warps = 3 per SM
+    // sub-partition, which leaves 170 registers per thread (no spills)
+    s.slices = (g.Nc + 351) / 352;
+    s.dcta = ((g.Nc + s.slices - 1) / s.slices + 31) / 32 * 32;
     s.threads = 32 + s.dcta;
     const int rowb = mode == MODE_F32C ? L.RW32 * 4 : L.RD64 * 8;
     const size_t fbytes = (size_t)g.N * (mode == MODE_F32C ? sizeof(float) : sizeof(double));
@@ -367,7 +366,7 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) return it->second;
     int base = (int)std::max<long long>(1, (long long)nsm / units);
-    int cand[4] = {base, 2 * base, 4 * base, 8 * base};
+    int cand[4] = {2 * base, 4 * base, 8 * base, 16 * base};
     float best_ms = 1e30f;
     int best = cand[1];
     cudaEvent_t e0, e1;
