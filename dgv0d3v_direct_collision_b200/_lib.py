@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdgv_b200.so")
 
 DGV_OK, DGV_EINVAL, DGV_ERANGE, DGV_ECUDA, DGV_ETIMEOUT, DGV_ENOMEM, DGV_ESTATE, DGV_EUNSUP = range(8)
-DGV_PREC_F64, DGV_PREC_F32C = 0, 1
+DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC = 0, 1, 2
 DGV_OPT_PROJECT, DGV_OPT_NCHUNKS = 1, 2
 
 STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4: "DGV_ETIMEOUT",

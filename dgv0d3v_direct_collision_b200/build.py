@@ -27,6 +27,7 @@ SOURCES = [
     ("layout.cpp", []),
     ("api.cu", []),
     ("collide.cu", []),
+    ("collide_tc.cu", []),
     ("adjoint.cu", []),
     ("noalloc.cu", []),
     ("synth.cu", ["-fmad=false"]),

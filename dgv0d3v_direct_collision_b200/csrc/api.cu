@@ -111,7 +111,8 @@ static void destroy_ctx(Ctx *c)
     cudaSetDevice(c->device);
     release_graphs(c);
     free_layout(c->lay);
-    double *bufs[] = {c->d_nu, c->d_nv, c->d_nw, c->d_nwt, c->d_partial, c->d_in, c->d_out, c->d_red, c->d_fm};
+    double *bufs[] = {c->d_nu, c->d_nv, c->d_nw, c->d_nwt, c->d_partial, c->d_in, c->d_out, c->d_red, c->d_fm,
+                      c->d_tcF, c->d_tcQ};
     for (double *p : bufs)
         if (p) cudaFree(p);
     for (double *p : c->d_tmp)

@@ -392,6 +392,7 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
 int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, double scale)
 {
     if (!c->lay.blk) return set_err(c, DGV_ESTATE, "collide: no A-arrays loaded");
+    if (precision == DGV_PREC_TC) return collide_tc_device(c, d_f, d_q, nvdf, scale);
     if (precision != DGV_PREC_F64 && precision != DGV_PREC_F32C)
         return set_err(c, DGV_EINVAL, "collide: unknown precision");
     int nch = choose_chunks(c, d_f, nullptr, d_q, nvdf, precision);

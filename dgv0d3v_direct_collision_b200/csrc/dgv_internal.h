@@ -63,6 +63,14 @@ struct Layout {
     std::vector<double> h_work;       // per block: pairs x valid shifts
     // work partitions: nchunks -> device array of nchunks+1 block bounds
     std::map<int, int *> chunks;
+    // tensor-core form (built on first use): per block ceil(count/64) chunk
+    // records of split-fp16 value tiles, their first record per block, the
+    // power-of-two value scale, and the block sets of one launch each
+    void *tc_V = nullptr;            // device
+    int *tc_chunk_start = nullptr;   // device, nblocks+1
+    double tc_vscale = 1.0;
+    std::vector<int> tc_chunk_host;
+    std::vector<int> tc_sets;
 };
 void free_layout(Layout &L);
 
@@ -87,6 +95,9 @@ struct Ctx {
     size_t tmp_n = 0;
     double *d_red = nullptr;  // reduction scratch
     size_t red_bytes = 0;
+    // tensor-core path: scaled fp32 copy of f (+ per-VDF scales), FP64 sums
+    double *d_tcF = nullptr, *d_tcQ = nullptr;
+    size_t tcF_bytes = 0, tcQ_bytes = 0;
     // Adams-Bashforth history: right sides frhs1..frhs5 (newest first)
     double *d_hist[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     int ab_order = 0;
@@ -125,6 +136,7 @@ int get_chunks(Ctx *c, int nchunks, int **d_bounds);
 // kernels (device pointers, ctx stream)
 int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision,
                    double scale);
+int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale);
 int jvp_device(Ctx *c, const double *d_f, const double *d_df, double *d_q, int precision);
 int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int precision);
 int moments_device(Ctx *c, const double *d_f, int nvdf, double *h_out);

@@ -26,6 +26,8 @@ void free_layout(Layout &L)
     if (L.rows64) cudaFree(L.rows64);
     if (L.rows32) cudaFree(L.rows32);
     for (auto &kv : L.chunks) cudaFree(kv.second);
+    if (L.tc_V) cudaFree(L.tc_V);
+    if (L.tc_chunk_start) cudaFree(L.tc_chunk_start);
     L = Layout();
 }
 

@@ -52,15 +52,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait for the completion of the phase with the given parity
+// bounded wait for the completion of the phase with the given parity.  While
+// waiting it also looks at the error flag about once a millisecond, so once
+// one wait has given up the other waits of the launch (and of launches queued
+// behind it) give up within a millisecond instead of each running its limit.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
+    unsigned long long tcheck = t0;
     while (!mbar_try_wait(bar, parity)) {
-        if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+        const unsigned long long t = globaltimer_ns();
+        if (t - t0 > WAIT_LIMIT_NS) {
             *(volatile int *)err = 1;  // host-mapped flag, read after the stream synchronises
             return false;
+        }
+        if (t - tcheck > 1000000ULL) {
+            tcheck = t;
+            if (*(volatile int *)err) return false;
         }
     }
     return true;

@@ -27,9 +27,9 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_OPT_PROJECT, DGV_OPT_NCHUNKS
+from ._lib import DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC, DGV_OPT_PROJECT, DGV_OPT_NCHUNKS
 
-PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C}
+PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C, "tc": DGV_PREC_TC}
 
 
 def _ptr(a):

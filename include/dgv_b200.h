@@ -45,6 +45,9 @@ extern "C" {
 /* arithmetic of the collision kernel */
 #define DGV_PREC_F64 0  /* plain FP64 gather-multiply-accumulate               */
 #define DGV_PREC_F32C 1 /* FP32 products, compensated (two-sum) accumulation   */
+#define DGV_PREC_TC 2   /* tensor cores (tcgen05): split-fp16 hi+lo products,  */
+                        /* FP32 accumulation, compensated per-block flush,     */
+                        /* FP64 final sums; at most 32 nodes per cell          */
 
 /* options for dgv_set_option */
 #define DGV_OPT_PROJECT 1  /* 1: apply the FP64 conservation projection to Q  */
