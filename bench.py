@@ -306,9 +306,11 @@ def run_ours(args, world, rank, local):
 
 
 def run_profile_case(case: str):
-    """Small case for profiler captures: one VDF on the 21^3 grid (s=3, M=7,
-    [-6,6]^3; A rows ~5.6 GB in total), fixed chunk count (no tuning
-    launches): one warm-up evaluation, then one evaluation to capture."""
+    """Small case for profiler captures on the 21^3 grid (s=3, M=7, [-6,6]^3;
+    A rows ~5.6 GB in total): one VDF with a fixed chunk count (no tuning
+    launches) for the CUDA-core kernels, a batch of 256 VDFs for the
+    tensor-core kernel (one launch per block set); one warm-up evaluation,
+    then one evaluation to capture."""
     import torch
 
     import dgv0d3v_direct_collision_b200 as dgv
@@ -316,8 +318,9 @@ def run_profile_case(case: str):
     s = dgv.DGVSolver(3, 7, 6.0)
     s.generate_synthetic_A(seed=SEED_A, support=1)
     s.set_nchunks(296)
-    fb = mixture_batch(s.nodes_u, s.nodes_v, s.nodes_w, s.nodes_gwts, 1, 3)
-    f = torch.tensor(fb[0], dtype=torch.float64, device="cuda")
+    nb = BATCH if prec == "tc" else 1
+    fb = mixture_batch(s.nodes_u, s.nodes_v, s.nodes_w, s.nodes_gwts, nb, 3)
+    f = torch.tensor(fb if nb > 1 else fb[0], dtype=torch.float64, device="cuda")
     q = torch.empty_like(f)
     times = []
     for _ in range(2):
@@ -333,7 +336,7 @@ def run_profile_case(case: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21"], default=None,
+    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21"], default=None,
                     help="small single-VDF case for profiler captures (no JSON bench line)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)

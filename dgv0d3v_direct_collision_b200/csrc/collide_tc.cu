@@ -4,8 +4,12 @@
 // two small matrices:  Q[(D,b), p] += sum_k  P[(D,b), k] * V[k, p],
 //   P[(D,b), k] = f_b(c1+D-ccell, l1_k) * f_b(c2+D-ccell, l2_k)   (k = pair)
 //   V[k, p]     = A value of canonical basis function p for pair k.
-// One tcgen05.mma tile has M = 128 rows = 4 consecutive output cells x 32
-// VDFs, N = 32 basis functions (P <= 32, zero-padded), K = 16 pairs.
+// One tcgen05.mma tile has M = 128 rows = NDG consecutive output cells x VB
+// VDFs (VB = 128, 64 or 32 by batch size), N = 32 basis functions (P <= 32,
+// zero-padded), K = 16 pairs.  A CTA owns one row tile for the blocks of one
+// launch; its A-values arrive as 64-pair chunk records (TMA bulk copies,
+// shared by every CTA of the launch through L2), and the f values of the
+// block's 2 x NDG cells are staged in shared memory once per block.
 //
 // Precision: P and V are split into fp16 hi + lo parts (x = hi + lo + O(2^-24 x))
 // after exact power-of-two scaling (per VDF for f, one global factor for A).
@@ -17,10 +21,11 @@
 // to the output accumulator in global memory.
 //
 // Warp roles (448 threads, one CTA per SM):
-//   warp 0      producer: TMA bulk copies of the V chunk records into a ring
+//   warp 0      producer: TMA bulk copies of f slices and V chunk records
 //   warp 1      allocates tensor memory; lane 0 issues the MMAs
-//   warps 2-9   generators: P tiles (split fp16) into shared memory
-//   warps 10-13 epilogue: per-block compensated flush, final FP64 add
+//   warps 2-9   generators: warp w writes k-group w (8 pairs) of the P tiles
+//               (split fp16) for all 128 rows
+//   warps 10-13 epilogue: chunk and block sums, final FP64 add
 // Every wait is bounded (%globaltimer); a timeout raises the error flag, each
 // role still reaches the final barrier, in-flight copies and MMAs are
 // drained, and tensor memory is freed before the CTA exits.
@@ -30,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
 #include "dgv_internal.h"
@@ -37,15 +43,16 @@
 
 namespace dgv {
 
-constexpr int TC_KCH = 64;                        // pairs per chunk record
-constexpr int TC_TILE_B = 32 * TC_KCH * 2;        // one 32 x 64 fp16 tile (4 KiB)
+constexpr int TC_KCH = 64;                          // pairs per chunk record
+constexpr int TC_TILE_B = 32 * TC_KCH * 2;          // one 32 x 64 fp16 tile (4 KiB)
 constexpr int TC_REC = 2 * TC_TILE_B + TC_KCH * 2;  // hi tile, lo tile, (l1,l2) bytes
 constexpr int TC_ROWS = 128;
-constexpr int TC_ATILE = TC_ROWS * TC_KCH * 2;    // 128 x 64 fp16 (16 KiB)
-constexpr int TC_NSTB = 4;                        // V ring stages
+constexpr int TC_ATILE = TC_ROWS * TC_KCH * 2;      // 128 x 64 fp16 (16 KiB)
+constexpr int TC_NSTB = 6;                          // V ring stages
 constexpr int TC_THREADS = 448;
 constexpr int TC_GEN_WARPS = 8;
 constexpr int TC_EPI_WARPS = 4;
+static_assert(TC_GEN_WARPS * 8 == TC_KCH, "one generator warp per k-group of 8 pairs");
 
 // ----------------------------------------------------------------------------
 // tcgen05 helpers (sm_100a)
@@ -124,23 +131,27 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_
 }
 
 struct TcArgs {
-    const float *F;           // [nbt][Nc][P][32] scaled f, zero for padded VDFs
+    const float *F;           // [nbt][Nc][P][VB] scaled f, zero for padded VDFs
     const unsigned char *V;   // chunk records
     const int *chunk_start;   // [nblocks+1]
     const BlockInfo *blk;
+    const int *order;         // row-tile order of this launch (heaviest first)
     double *qacc;             // [(D*P+p)*NV + vdf]
     const double *inv_scale;  // [NV]
     int *err;
     int b0, b1;               // block range of this launch
-    int Nc, P, Mv, Mw, ccell, NV, nvdf;
+    int Nc, P, Mv, Mw, ccell, NV, nvdf, nbt;
+    int off_f, fslot;         // shared-memory offset and size of one f slot
 };
 
+template <int NDG>
 __device__ __forceinline__ bool dgroup_meets(const BlockInfo &bi, int D0, int Nc, int Mv, int Mw)
 {
-    for (int d = 0; d < 4; d++) {
-        int D = D0 + d;
+#pragma unroll
+    for (int d = 0; d < NDG; d++) {
+        const int D = D0 + d;
         if (D >= Nc) break;
-        int Du = D / (Mv * Mw), Dv = (D / Mw) % Mv, Dw = D % Mw;
+        const int Du = D / (Mv * Mw), Dv = (D / Mw) % Mv, Dw = D % Mw;
         if (Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] && Dw >= bi.lo[2] &&
             Dw <= bi.hi[2])
             return true;
@@ -154,25 +165,27 @@ __device__ __forceinline__ bool dgroup_meets(const BlockInfo &bi, int D0, int Nc
 // Tensor memory (256 columns): hi*hi accumulators of chunks (double
 // buffered, columns 0-31 / 32-63), hi*lo + lo*hi accumulators of blocks
 // (64-95 / 96-127), compensated sum and correction (128-159 / 160-191).
-// The hi*hi chain of a chunk is only 4 MMAs long and the small terms get
-// their own chain, so few roundings of the tensor-core accumulator reach
-// the result; chunk sums are added in FP32 (round to nearest) and block sums
-// with two-sum.
+template <int VB>
 __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
 {
+    constexpr int NDG = TC_ROWS / VB;  // output cells per row tile
+    constexpr int NJ = VB / 32;        // VDF groups of 32 per output cell
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *abuf = smem;                                // 2 x (hi, lo) A tiles
-    unsigned char *vring = smem + 4 * TC_ATILE;                // TC_NSTB x TC_REC
-    uint64_t *bars = reinterpret_cast<uint64_t *>(vring + TC_NSTB * TC_REC);
+    unsigned char *abuf = smem;                   // 2 x (hi, lo) A tiles
+    unsigned char *vring = smem + 4 * TC_ATILE;   // TC_NSTB x TC_REC
+    float *fs = reinterpret_cast<float *>(smem + a.off_f);  // 2 slots x {side 1, side 2}
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + a.off_f + 2 * a.fslot);
     uint64_t *b_full = bars, *b_empty = bars + TC_NSTB;
     uint64_t *a_full = bars + 2 * TC_NSTB, *a_empty = a_full + 2;
-    uint64_t *h_full = a_empty + 2, *h_empty = h_full + 2;     // chunk accumulators
-    uint64_t *l_full = h_empty + 2, *l_empty = l_full + 2;     // block accumulators
-    uint64_t *drain = l_empty + 2;
+    uint64_t *h_full = a_empty + 2, *h_empty = h_full + 2;  // chunk accumulators
+    uint64_t *l_full = h_empty + 2, *l_empty = l_full + 2;  // block accumulators
+    uint64_t *f_full = l_empty + 2, *f_empty = f_full + 2;  // f slots
+    uint64_t *drain = f_empty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bt = blockIdx.x, D0 = blockIdx.y * 4;
+    const int bt = blockIdx.x % a.nbt, D0 = a.order[blockIdx.x / a.nbt] * NDG;
+    const int cell_floats = a.P * VB;  // one cell of one VDF tile
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_NSTB; s++) {
             mbar_init(&b_full[s], 1);
@@ -185,6 +198,8 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
             mbar_init(&h_empty[s], TC_EPI_WARPS);
             mbar_init(&l_full[s], 1);
             mbar_init(&l_empty[s], TC_EPI_WARPS);
+            mbar_init(&f_full[s], 1);
+            mbar_init(&f_empty[s], TC_GEN_WARPS);
         }
         mbar_init(drain, 1);
         fence_mbar_init();
@@ -205,11 +220,37 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
     if (warp == 0) {
         // ---------------- producer ----------------
         if (lane == 0) {
-            int g = 0;
+            int g = 0, q = 0;
             bool ok = true;
+            const float *Fbt = a.F + (size_t)bt * a.Nc * cell_floats;
             for (int b = a.b0; b < a.b1 && ok; b++) {
                 const BlockInfo bi = a.blk[b];
-                if (!dgroup_meets(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
+                if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
+                // f of cells c1 + D - ccell and c2 + D - ccell, D in the tile,
+                // clipped to the grid (cells outside are never read)
+                const int fb = q & 1;
+                if (!mbar_wait(&f_empty[fb], ((q >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
+                int lo[2], hi[2];
+                uint32_t tx = 0;
+                for (int sd = 0; sd < 2; sd++) {
+                    const int cs = (sd ? bi.c2 : bi.c1) + D0 - a.ccell;
+                    lo[sd] = max(cs, 0);
+                    hi[sd] = min(cs + NDG, a.Nc);
+                    if (hi[sd] > lo[sd]) tx += (uint32_t)((hi[sd] - lo[sd]) * cell_floats * 4);
+                }
+                if (tx) {
+                    mbar_arrive_expect_tx(&f_full[fb], tx);
+                    for (int sd = 0; sd < 2; sd++) {
+                        if (hi[sd] <= lo[sd]) continue;
+                        const int cs = (sd ? bi.c2 : bi.c1) + D0 - a.ccell;
+                        float *dst = fs + (size_t)(2 * fb + sd) * NDG * cell_floats + (size_t)(lo[sd] - cs) * cell_floats;
+                        bulk_g2s(dst, Fbt + (size_t)lo[sd] * cell_floats, (uint32_t)((hi[sd] - lo[sd]) * cell_floats * 4),
+                                 &f_full[fb]);
+                    }
+                } else {
+                    mbar_arrive(&f_full[fb]);
+                }
+                q++;
                 const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
                 for (int c = c0; c < c1; c++, g++) {
                     const int s = g % TC_NSTB;
@@ -218,9 +259,11 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
                     bulk_g2s(vring + s * TC_REC, a.V + (size_t)c * TC_REC, TC_REC, &b_full[s]);
                 }
             }
-            if (!ok)  // let the copies already issued land
+            if (!ok) {  // let the copies already issued land
                 for (int j = g > TC_NSTB ? g - TC_NSTB : 0; j < g; j++)
                     mbar_wait(&b_full[j % TC_NSTB], (j / TC_NSTB) & 1, a.err);
+                for (int j = q > 2 ? q - 2 : 0; j < q; j++) mbar_wait(&f_full[j & 1], (j >> 1) & 1, a.err);
+            }
         }
         __syncwarp();
     } else if (warp == 1) {
@@ -230,7 +273,7 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
             bool ok = true;
             for (int b = a.b0; b < a.b1 && ok; b++) {
                 const BlockInfo bi = a.blk[b];
-                if (!dgroup_meets(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
+                if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
                 const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
                 const int lb = q & 1;
                 if (!mbar_wait(&l_empty[lb], ((q >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
@@ -268,53 +311,72 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
         __syncwarp();
     } else if (warp < 2 + TC_GEN_WARPS) {
         // ---------------- generators ----------------
-        const int gi = warp - 2, d = gi & 3, kh = gi >> 2;  // output cell slot, half of the chunk
-        const int D = D0 + d, row = d * 32 + lane;
-        const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
-        const float *Fb = a.F + (size_t)bt * a.Nc * a.P * 32 + lane;
-        int g = 0;
+        const int kg = warp - 2;  // k-group of this warp: pairs 8 kg .. 8 kg + 7 of a chunk
+        int Dc[NDG];
+#pragma unroll
+        for (int d = 0; d < NDG; d++) Dc[d] = D0 + d;
+        int g = 0, q = 0;
         bool ok = true;
         for (int b = a.b0; b < a.b1 && ok; b++) {
             const BlockInfo bi = a.blk[b];
-            if (!dgroup_meets(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
-            const bool valid = D < a.Nc && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
-                               Dw >= bi.lo[2] && Dw <= bi.hi[2];
-            const float *F1 = Fb + (size_t)(bi.c1 + D - a.ccell) * a.P * 32;
-            const float *F2 = Fb + (size_t)(bi.c2 + D - a.ccell) * a.P * 32;
+            if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
+            bool valid[NDG];
+#pragma unroll
+            for (int d = 0; d < NDG; d++) {
+                const int D = Dc[d];
+                const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
+                valid[d] = D < a.Nc && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
+                           Dw >= bi.lo[2] && Dw <= bi.hi[2];
+            }
+            const int fb = q & 1;
+            if (!mbar_wait_warp(&f_full[fb], (q >> 1) & 1, a.err)) { ok = false; break; }
+            const float *f1 = fs + (size_t)(2 * fb) * NDG * cell_floats + lane;
+            const float *f2 = f1 + (size_t)NDG * cell_floats;
             const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
             for (int c = c0; c < c1; c++, g++) {
                 const int s = g % TC_NSTB, x = g & 1;
                 if (!mbar_wait_warp(&b_full[s], (g / TC_NSTB) & 1, a.err)) { ok = false; break; }
                 if (!mbar_wait_warp(&a_empty[x], ((g >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
-                const unsigned char *idx = vring + s * TC_REC + 2 * TC_TILE_B;
+                const uint4 iv = *reinterpret_cast<const uint4 *>(vring + s * TC_REC + 2 * TC_TILE_B + 16 * kg);
+                const uint32_t w4[4] = {iv.x, iv.y, iv.z, iv.w};
+                int o1[8], o2[8];  // f offsets (floats) of the 8 pairs
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const uint32_t wd = w4[j >> 1] >> (16 * (j & 1));
+                    o1[j] = (int)(wd & 0xffu) * VB;
+                    o2[j] = (int)((wd >> 8) & 0xffu) * VB;
+                }
                 unsigned char *ah = abuf + (2 * x) * TC_ATILE, *al = abuf + (2 * x + 1) * TC_ATILE;
 #pragma unroll
-                for (int kgl = 0; kgl < 4; kgl++) {
-                    const int kg = kh * 4 + kgl;
-                    uint32_t hi[4], lo[4];
-                    if (valid) {
-                        float x8[8];
+                for (int d = 0; d < NDG; d++) {
+                    const float *p1 = f1 + d * cell_floats, *p2 = f2 + d * cell_floats;
 #pragma unroll
-                        for (int j = 0; j < 8; j++) {
-                            const int k = kg * 8 + j;
-                            const int l1 = idx[2 * k], l2 = idx[2 * k + 1];
-                            x8[j] = __ldg(F1 + l1 * 32) * __ldg(F2 + l2 * 32);
+                    for (int jj = 0; jj < NJ; jj++) {
+                        const int row = d * VB + jj * 32 + lane;
+                        uint32_t hi[4], lo[4];
+                        if (valid[d]) {
+                            float x8[8];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) x8[j] = p1[o1[j] + jj * 32] * p2[o2[j] + jj * 32];
+#pragma unroll
+                            for (int j = 0; j < 4; j++) split2(x8[2 * j], x8[2 * j + 1], hi[j], lo[j]);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 4; j++) { hi[j] = 0u; lo[j] = 0u; }
                         }
-#pragma unroll
-                        for (int j = 0; j < 4; j++) split2(x8[2 * j], x8[2 * j + 1], hi[j], lo[j]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < 4; j++) { hi[j] = 0u; lo[j] = 0u; }
+                        // core matrix (row/8, kg): 8 rows x 16 bytes
+                        const int off = ((row >> 3) * 8 + kg) * 128 + (row & 7) * 16;
+                        *reinterpret_cast<uint4 *>(ah + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                        *reinterpret_cast<uint4 *>(al + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
                     }
-                    // core matrix (row/8, kg): 8 rows x 16 bytes
-                    const int off = ((row >> 3) * 8 + kg) * 128 + (row & 7) * 16;
-                    *reinterpret_cast<uint4 *>(ah + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                    *reinterpret_cast<uint4 *>(al + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
                 }
                 fence_async_shared();  // generic-proxy writes -> visible to the tensor core
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&a_full[x]);
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&f_empty[fb]);  // this warp's reads of the f slot are done
+            q++;
         }
     } else if (warp < 2 + TC_GEN_WARPS + TC_EPI_WARPS) {
         // ---------------- epilogue ----------------
@@ -329,7 +391,7 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
         bool ok = true;
         for (int b = a.b0; b < a.b1 && ok; b++) {
             const BlockInfo bi = a.blk[b];
-            if (!dgroup_meets(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
+            if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
             const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
             for (int c = c0; c < c1; c++, g++) {
                 const int x = g & 1;
@@ -373,7 +435,7 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
             q++;
         }
         if (ok) {
-            const int d = r >> 5, vdf = bt * 32 + (r & 31);
+            const int d = r / VB, vdf = bt * VB + (r % VB);
             const int D = D0 + d;
             const bool mine = D < a.Nc && vdf < a.nvdf;
             const double sc = mine ? a.inv_scale[vdf] : 0.0;
@@ -447,9 +509,10 @@ __global__ void k_absmax_rows(const double *rows64, long long npairs, int RD64, 
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
-// per-VDF scale 2^e (max |f| -> 2^6) and the scaled, b-minor copy of f
+// per-VDF scale 2^e (max |f| -> [32, 64)) and the scaled copy of f in VDF
+// tiles of VB: F[((bt*Nc + cell)*P + l)*VB + v%VB]
 __global__ void k_tc_fprep(const double *f, long long N, int nvdf, double vinv, float *F, double *inv_scale,
-                           int Nc, int P, int NV)
+                           int Nc, int P, int VB)
 {
     const int v = blockIdx.x;
     __shared__ double red[32];
@@ -473,11 +536,11 @@ __global__ void k_tc_fprep(const double *f, long long N, int nvdf, double vinv, 
     }
     const double s = ldexp(1.0, e);
     if (threadIdx.x == 0) inv_scale[v] = ldexp(1.0, -2 * e) * vinv;
-    const int bt = v / 32, lb = v % 32;
+    const int bt = v / VB, lb = v % VB;
     for (long long i = threadIdx.x; i < N; i += blockDim.x) {
         const int cell = (int)(i / P), l = (int)(i - (long long)cell * P);
         const double x = v < nvdf ? f[(size_t)v * N + i] * s : 0.0;
-        F[(((size_t)bt * Nc + cell) * P + l) * 32 + lb] = (float)x;
+        F[(((size_t)bt * Nc + cell) * P + l) * VB + lb] = (float)x;
     }
 }
 
@@ -516,7 +579,7 @@ static int tc_prepare(Ctx *c)
     int e = 0;
     if (vmax > 0.0) {
         std::frexp(vmax, &e);
-        e = 14 - e;
+        e = 14 - e;  // largest |value| -> [2^13, 2^14): fp16 hi parts stay finite
     }
     L.tc_vscale = std::ldexp(1.0, e);
     DGV_CUDA(c, cudaMalloc(&L.tc_chunk_start, sizeof(int) * (L.nblocks + 1)));
@@ -528,7 +591,8 @@ static int tc_prepare(Ctx *c)
                                                                 (float)L.tc_vscale, (unsigned char *)L.tc_V);
     DGV_CUDA(c, cudaGetLastError());
     L.tc_chunk_host = cs;
-    // block sets of about 48 MB of chunk records each (their values stay in L2)
+    // block sets of about 48 MB of chunk records each: one launch per set, its
+    // records stay in L2 while every row tile reads them
     L.tc_sets.clear();
     L.tc_sets.push_back(0);
     const long long per_set = (48LL << 20) / TC_REC;
@@ -541,41 +605,101 @@ static int tc_prepare(Ctx *c)
     return DGV_OK;
 }
 
+// Row-tile order per launch: tiles (groups of NDG output cells) sorted by the
+// chunk records they consume, heaviest first, so the last wave of CTAs is
+// short.  One array of nsets x ngroups on the device, built once per NDG.
+static int tc_order(Ctx *c, int NDG, const int **d_order)
+{
+    Layout &L = c->lay;
+    auto it = L.tc_order.find(NDG);
+    if (it != L.tc_order.end()) { *d_order = it->second; return DGV_OK; }
+    const Grid &g = c->grid;
+    const int ng = (g.Nc + NDG - 1) / NDG, nsets = (int)L.tc_sets.size() - 1;
+    std::vector<int> all((size_t)nsets * ng);
+    std::vector<long long> work(ng);
+    std::vector<int> stamp(ng, -1);
+    for (int s = 0; s < nsets; s++) {
+        std::fill(work.begin(), work.end(), 0);
+        for (int b = L.tc_sets[s]; b < L.tc_sets[s + 1]; b++) {
+            const BlockInfo &bi = L.h_blk[b];
+            const int ch = L.tc_chunk_host[b + 1] - L.tc_chunk_host[b];
+            for (int u = bi.lo[0]; u <= bi.hi[0]; u++)
+                for (int v = bi.lo[1]; v <= bi.hi[1]; v++)
+                    for (int w = bi.lo[2]; w <= bi.hi[2]; w++) {
+                        const int grp = ((u * g.d.Mv + v) * g.d.Mw + w) / NDG;
+                        if (stamp[grp] != b) { stamp[grp] = b; work[grp] += ch; }
+                    }
+        }
+        int *o = all.data() + (size_t)s * ng;
+        std::iota(o, o + ng, 0);
+        std::stable_sort(o, o + ng, [&](int x, int y) { return work[x] > work[y]; });
+    }
+    int *d = nullptr;
+    DGV_CUDA(c, cudaMalloc(&d, sizeof(int) * all.size()));
+    DGV_CUDA(c, cudaMemcpy(d, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
+    L.tc_order[NDG] = d;
+    *d_order = d;
+    return DGV_OK;
+}
+
+template <int VB>
+static int launch_tc(Ctx *c, TcArgs &a, const int *d_order, int ng)
+{
+    const size_t smem = (size_t)a.off_f + 2 * (size_t)a.fslot + (2 * TC_NSTB + 20) * sizeof(uint64_t) + 16;
+    DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc<VB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    const Layout &L = c->lay;
+    for (size_t s = 0; s + 1 < L.tc_sets.size(); s++) {
+        a.b0 = L.tc_sets[s];
+        a.b1 = L.tc_sets[s + 1];
+        a.order = d_order + s * ng;
+        k_collide_tc<VB><<<(unsigned)(a.nbt * ng), TC_THREADS, smem, c->stream>>>(a);
+        DGV_CUDA(c, cudaGetLastError());
+    }
+    return DGV_OK;
+}
+
 int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
     if (!L.blk) return set_err(c, DGV_ESTATE, "collide: no A-arrays loaded");
     if (g.P > 32) return set_err(c, DGV_EUNSUP, "tensor-core path: at most 32 nodes per cell");
+    if (nvdf < 1) return set_err(c, DGV_EINVAL, "collide: batch must hold at least one VDF");
     int rc = tc_prepare(c);
     if (rc) return rc;
     rc = ensure_errflag(c);
     if (rc) return rc;
-    const int nbt = (nvdf + 31) / 32, NV = nbt * 32;
-    const size_t fbytes = (size_t)nbt * g.Nc * g.P * 32 * sizeof(float);
+    // VDFs per row tile: all 128 rows of a tile on one output cell when the
+    // batch fills them, else 2 or 4 consecutive cells
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), NDG = TC_ROWS / VB;
+    const int nbt = (nvdf + VB - 1) / VB, NV = nbt * VB, ng = (g.Nc + NDG - 1) / NDG;
+    const size_t fbytes = (size_t)nbt * g.Nc * g.P * VB * sizeof(float);
     const size_t qbytes = (size_t)g.N * NV * sizeof(double);
     rc = ensure_buffer(c, &c->d_tcF, &c->tcF_bytes, fbytes + NV * sizeof(double));
     if (rc) return rc;
     rc = ensure_buffer(c, &c->d_tcQ, &c->tcQ_bytes, qbytes);
     if (rc) return rc;
+    const int *d_order = nullptr;
+    rc = tc_order(c, NDG, &d_order);
+    if (rc) return rc;
     float *F = reinterpret_cast<float *>(c->d_tcF);
     double *inv = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_tcF) + fbytes);
-    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc_vscale, F, inv, g.Nc, g.P, NV);
+    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc_vscale, F, inv, g.Nc, g.P, VB);
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
-    const size_t smem = 4 * (size_t)TC_ATILE + (size_t)TC_NSTB * TC_REC + (2 * TC_NSTB + 16) * sizeof(uint64_t) + 16;
-    DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     TcArgs a;
     a.F = F; a.V = (const unsigned char *)L.tc_V; a.chunk_start = L.tc_chunk_start; a.blk = L.blk;
-    a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
-    a.Nc = g.Nc; a.P = g.P; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf;
-    const dim3 grid(nbt, (g.Nc + 3) / 4);
-    for (size_t s = 0; s + 1 < L.tc_sets.size(); s++) {
-        a.b0 = L.tc_sets[s];
-        a.b1 = L.tc_sets[s + 1];
-        k_collide_tc<<<grid, TC_THREADS, smem, c->stream>>>(a);
-        DGV_CUDA(c, cudaGetLastError());
+    a.order = nullptr; a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
+    a.Nc = g.Nc; a.P = g.P; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
+    a.off_f = 4 * TC_ATILE + TC_NSTB * TC_REC;                 // 16-byte aligned
+    a.fslot = 2 * NDG * g.P * VB * (int)sizeof(float);         // both sides of one block
+    switch (VB) {
+    case 128: rc = launch_tc<128>(c, a, d_order, ng); break;
+    case 64: rc = launch_tc<64>(c, a, d_order, ng); break;
+    default: rc = launch_tc<32>(c, a, d_order, ng); break;
     }
+    if (rc) return rc;
     long long tot = (long long)nvdf * g.N;
     k_tc_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, c->d_nwt, d_q, g.N, nvdf, NV, scale);
     DGV_CUDA(c, cudaGetLastError());

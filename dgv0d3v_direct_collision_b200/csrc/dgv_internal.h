@@ -71,6 +71,7 @@ struct Layout {
     double tc_vscale = 1.0;
     std::vector<int> tc_chunk_host;
     std::vector<int> tc_sets;
+    std::map<int, int *> tc_order;   // device row-tile orders, keyed by cells per tile
 };
 void free_layout(Layout &L);
 
