@@ -56,7 +56,7 @@ def _stale(obj: str, deps) -> bool:
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     nv = nvcc()
-    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "dgv_b200.h"))
     objs = []
     for src, extra in SOURCES:

@@ -45,10 +45,11 @@ namespace dgv {
 
 constexpr int TC_KCH = 64;                          // pairs per chunk record
 constexpr int TC_TILE_B = 32 * TC_KCH * 2;          // one 32 x 64 fp16 tile (4 KiB)
-constexpr int TC_REC = 2 * TC_TILE_B + TC_KCH * 2;  // hi tile, lo tile, (l1,l2) bytes
+constexpr int TC_REC = 2 * TC_TILE_B + TC_KCH * 4;  // hi tile, lo tile, f offsets of the pairs
 constexpr int TC_ROWS = 128;
+constexpr int TC_NSTB = 4;                          // V ring stages
+constexpr int TC_NA = 3;                            // A tile stages
 constexpr int TC_ATILE = TC_ROWS * TC_KCH * 2;      // 128 x 64 fp16 (16 KiB)
-constexpr int TC_NSTB = 6;                          // V ring stages
 constexpr int TC_THREADS = 448;
 constexpr int TC_GEN_WARPS = 8;
 constexpr int TC_EPI_WARPS = 4;
@@ -71,6 +72,18 @@ __device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t 
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
         "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+// A operand from tensor memory (lane = row, column = two consecutive K
+// elements, the lower K in the low half), B from shared memory
+__device__ __forceinline__ void umma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(db), "r"(idesc), "r"(acc)
         : "memory");
 }
 
@@ -112,12 +125,40 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float *v)
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
+// two FP32 products with one packed instruction (round to nearest, as FMUL)
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
 // bounded wait whose outcome is the same for every lane of the warp (the
 // warp-collective tensor-memory instructions that follow need a converged warp)
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, int *err)
 {
     const bool ok = mbar_wait(bar, parity, err);
     return __all_sync(0xffffffffu, ok);
+}
+
+__device__ __forceinline__ void tmem_st8u(uint32_t taddr, const uint32_t *r)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_st16u(uint32_t taddr, const uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
 }
 
 // split x into fp16 hi + lo (two values at a time)
@@ -130,74 +171,66 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_
     lo = *reinterpret_cast<uint32_t *>(&l);
 }
 
+// One entry of a row tile's work list: a block whose valid output-cell box
+// meets the tile, with its chunk records and the tile cells it is valid for.
+struct __align__(16) TcItem {
+    int chunk0;  // first chunk record
+    int nch;     // chunk records (bits 0-15) | valid cell slots of the tile << 16
+    int c1, c2;  // cells of the block, canonical frame
+};
+
 struct TcArgs {
     const float *F;           // [nbt][Nc][P][VB] scaled f, zero for padded VDFs
     const unsigned char *V;   // chunk records
-    const int *chunk_start;   // [nblocks+1]
-    const BlockInfo *blk;
-    const int *order;         // row-tile order of this launch (heaviest first)
+    const TcItem *items;      // work lists of this launch
+    const int *item_start;    // [ntiles + 1] into items, tiles in launch order
+    const int *tile_of;       // row-tile index (group of NDG cells) in launch order
     double *qacc;             // [(D*P+p)*NV + vdf]
     const double *inv_scale;  // [NV]
     int *err;
-    int b0, b1;               // block range of this launch
-    int Nc, P, Mv, Mw, ccell, NV, nvdf, nbt;
+    int Nc, P, ccell, NV, nvdf, nbt;
     int off_f, fslot;         // shared-memory offset and size of one f slot
 };
-
-template <int NDG>
-__device__ __forceinline__ bool dgroup_meets(const BlockInfo &bi, int D0, int Nc, int Mv, int Mw)
-{
-#pragma unroll
-    for (int d = 0; d < NDG; d++) {
-        const int D = D0 + d;
-        if (D >= Nc) break;
-        const int Du = D / (Mv * Mw), Dv = (D / Mw) % Mv, Dw = D % Mw;
-        if (Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] && Dw >= bi.lo[2] &&
-            Dw <= bi.hi[2])
-            return true;
-    }
-    return false;
-}
 
 // 512 in the launch bound caps registers at 128 per thread: with 14 warps,
 // two of the four SM sub-partitions hold 4 warps each.
 //
-// Tensor memory (256 columns): hi*hi accumulators of chunks (double
-// buffered, columns 0-31 / 32-63), hi*lo + lo*hi accumulators of blocks
-// (64-95 / 96-127), compensated sum and correction (128-159 / 160-191).
+// Tensor memory (256 columns): per chunk (double buffered, 64 columns each)
+// hi*hi in the first 32 columns and hi*lo + lo*hi in the next 32; the
+// compensated sum and its correction in columns 128-159 / 160-191.
 template <int VB>
 __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
 {
     constexpr int NDG = TC_ROWS / VB;  // output cells per row tile
-    constexpr int NJ = VB / 32;        // VDF groups of 32 per output cell
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *abuf = smem;                   // 2 x (hi, lo) A tiles
-    unsigned char *vring = smem + 4 * TC_ATILE;   // TC_NSTB x TC_REC
+    unsigned char *abuf = smem;                          // TC_NA x (hi, lo) A tiles
+    unsigned char *vring = smem + 2 * TC_NA * TC_ATILE;  // TC_NSTB x TC_REC
     float *fs = reinterpret_cast<float *>(smem + a.off_f);  // 2 slots x {side 1, side 2}
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + a.off_f + 2 * a.fslot);
     uint64_t *b_full = bars, *b_empty = bars + TC_NSTB;
-    uint64_t *a_full = bars + 2 * TC_NSTB, *a_empty = a_full + 2;
-    uint64_t *h_full = a_empty + 2, *h_empty = h_full + 2;  // chunk accumulators
-    uint64_t *l_full = h_empty + 2, *l_empty = l_full + 2;  // block accumulators
-    uint64_t *f_full = l_empty + 2, *f_empty = f_full + 2;  // f slots
+    uint64_t *a_full = bars + 2 * TC_NSTB, *a_empty = a_full + TC_NA;
+    uint64_t *h_full = a_empty + TC_NA, *h_empty = h_full + 2;  // chunk accumulators
+    uint64_t *f_full = h_empty + 2, *f_empty = f_full + 2;      // f slots
     uint64_t *drain = f_empty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bt = blockIdx.x % a.nbt, D0 = a.order[blockIdx.x / a.nbt] * NDG;
+    const int bt = blockIdx.x % a.nbt, ti = blockIdx.x / a.nbt;
+    const int D0 = a.tile_of[ti] * NDG;
+    const int i0 = a.item_start[ti], i1 = a.item_start[ti + 1];
     const int cell_floats = a.P * VB;  // one cell of one VDF tile
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_NSTB; s++) {
             mbar_init(&b_full[s], 1);
             mbar_init(&b_empty[s], 1);
         }
-        for (int s = 0; s < 2; s++) {
+        for (int s = 0; s < TC_NA; s++) {
             mbar_init(&a_full[s], TC_GEN_WARPS);
             mbar_init(&a_empty[s], 1);
+        }
+        for (int s = 0; s < 2; s++) {
             mbar_init(&h_full[s], 1);
             mbar_init(&h_empty[s], TC_EPI_WARPS);
-            mbar_init(&l_full[s], 1);
-            mbar_init(&l_empty[s], TC_EPI_WARPS);
             mbar_init(&f_full[s], 1);
             mbar_init(&f_empty[s], TC_GEN_WARPS);
         }
@@ -213,9 +246,6 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    // instruction descriptor: FP32 accumulator, fp16 A and B, both K-major,
-    // N = 32, M = 128
-    const uint32_t idesc = (1u << 4) | ((uint32_t)(32 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 
     if (warp == 0) {
         // ---------------- producer ----------------
@@ -223,9 +253,8 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
             int g = 0, q = 0;
             bool ok = true;
             const float *Fbt = a.F + (size_t)bt * a.Nc * cell_floats;
-            for (int b = a.b0; b < a.b1 && ok; b++) {
-                const BlockInfo bi = a.blk[b];
-                if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
+            for (int it = i0; it < i1 && ok; it++) {
+                const TcItem e = a.items[it];
                 // f of cells c1 + D - ccell and c2 + D - ccell, D in the tile,
                 // clipped to the grid (cells outside are never read)
                 const int fb = q & 1;
@@ -233,7 +262,7 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
                 int lo[2], hi[2];
                 uint32_t tx = 0;
                 for (int sd = 0; sd < 2; sd++) {
-                    const int cs = (sd ? bi.c2 : bi.c1) + D0 - a.ccell;
+                    const int cs = (sd ? e.c2 : e.c1) + D0 - a.ccell;
                     lo[sd] = max(cs, 0);
                     hi[sd] = min(cs + NDG, a.Nc);
                     if (hi[sd] > lo[sd]) tx += (uint32_t)((hi[sd] - lo[sd]) * cell_floats * 4);
@@ -242,7 +271,7 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
                     mbar_arrive_expect_tx(&f_full[fb], tx);
                     for (int sd = 0; sd < 2; sd++) {
                         if (hi[sd] <= lo[sd]) continue;
-                        const int cs = (sd ? bi.c2 : bi.c1) + D0 - a.ccell;
+                        const int cs = (sd ? e.c2 : e.c1) + D0 - a.ccell;
                         float *dst = fs + (size_t)(2 * fb + sd) * NDG * cell_floats + (size_t)(lo[sd] - cs) * cell_floats;
                         bulk_g2s(dst, Fbt + (size_t)lo[sd] * cell_floats, (uint32_t)((hi[sd] - lo[sd]) * cell_floats * 4),
                                  &f_full[fb]);
@@ -251,12 +280,12 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
                     mbar_arrive(&f_full[fb]);
                 }
                 q++;
-                const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
-                for (int c = c0; c < c1; c++, g++) {
+                const int nch = e.nch & 0xffff;
+                for (int c = 0; c < nch; c++, g++) {
                     const int s = g % TC_NSTB;
                     if (!mbar_wait(&b_empty[s], ((g / TC_NSTB) & 1) ^ 1, a.err)) { ok = false; break; }
                     mbar_arrive_expect_tx(&b_full[s], TC_REC);
-                    bulk_g2s(vring + s * TC_REC, a.V + (size_t)c * TC_REC, TC_REC, &b_full[s]);
+                    bulk_g2s(vring + s * TC_REC, a.V + (size_t)(e.chunk0 + c) * TC_REC, TC_REC, &b_full[s]);
                 }
             }
             if (!ok) {  // let the copies already issued land
@@ -269,40 +298,37 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            int g = 0, q = 0;
+            // instruction descriptors: FP32 accumulator, fp16 A and B, both
+            // K-major, M = 128, N = 64 (B hi and lo tiles: hi*hi and hi*lo in
+            // one instruction) or N = 32 (B hi tile: lo*hi)
+            const uint32_t id64 = (1u << 4) | ((uint32_t)(64 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+            const uint32_t id32 = (1u << 4) | ((uint32_t)(32 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+            const uint64_t dA0 = umma_desc(smem_u32(abuf), 128, 1024);
+            const uint64_t dV0 = umma_desc(smem_u32(vring), 128, 1024);
+            int g = 0;
             bool ok = true;
-            for (int b = a.b0; b < a.b1 && ok; b++) {
-                const BlockInfo bi = a.blk[b];
-                if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
-                const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
-                const int lb = q & 1;
-                if (!mbar_wait(&l_empty[lb], ((q >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
-                const uint32_t dlo = tmem + (uint32_t)(64 + lb * 32);
-                for (int c = c0; c < c1; c++, g++) {
-                    const int s = g % TC_NSTB, x = g & 1;
+            for (int it = i0; it < i1 && ok; it++) {
+                const int nch = a.items[it].nch & 0xffff;
+                for (int c = 0; c < nch; c++, g++) {
+                    const int s = g % TC_NSTB, xa = g % TC_NA, xh = g & 1;
                     if (!mbar_wait(&b_full[s], (g / TC_NSTB) & 1, a.err)) { ok = false; break; }
-                    if (!mbar_wait(&a_full[x], (g >> 1) & 1, a.err)) { ok = false; break; }
-                    if (!mbar_wait(&h_empty[x], ((g >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
+                    if (!mbar_wait(&a_full[xa], (g / TC_NA) & 1, a.err)) { ok = false; break; }
+                    if (!mbar_wait(&h_empty[xh], ((g >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t dhi = tmem + (uint32_t)(x * 32);
-                    const uint32_t vb = smem_u32(vring + s * TC_REC);
-                    const uint32_t ah = smem_u32(abuf + (2 * x) * TC_ATILE), al = smem_u32(abuf + (2 * x + 1) * TC_ATILE);
+                    const uint32_t dacc = tmem + (uint32_t)(xh * 64);
+                    // descriptor start addresses are in 16-byte units
+                    const uint64_t dAh = dA0 + (uint64_t)((2 * xa) * TC_ATILE >> 4);
+                    const uint64_t dAl = dA0 + (uint64_t)((2 * xa + 1) * TC_ATILE >> 4);
+                    const uint64_t dB = dV0 + (uint64_t)(s * TC_REC >> 4);
 #pragma unroll
-                    for (int t = 0; t < TC_KCH / 16; t++) {
-                        const uint32_t ko = t * 256;  // two core matrices (K = 16) per step
-                        const uint64_t dAh = umma_desc(ah + ko, 128, 1024), dAl = umma_desc(al + ko, 128, 1024);
-                        const uint64_t dBh = umma_desc(vb + ko, 128, 1024), dBl = umma_desc(vb + TC_TILE_B + ko, 128, 1024);
-                        umma_f16(dhi, dAh, dBh, idesc, t == 0 ? 0u : 1u);
-                        umma_f16(dlo, dAh, dBl, idesc, (c == c0 && t == 0) ? 0u : 1u);
-                        umma_f16(dlo, dAl, dBh, idesc, 1u);
+                    for (int t = 0; t < TC_KCH / 16; t++) {  // K = 16: two core matrices (256 B) per step
+                        umma_f16(dacc, dAh + 16 * t, dB + 16 * t, id64, t == 0 ? 0u : 1u);
+                        umma_f16(dacc + 32, dAl + 16 * t, dB + 16 * t, id32, 1u);
                     }
-                    umma_commit(&a_empty[x]);
+                    umma_commit(&a_empty[xa]);
                     umma_commit(&b_empty[s]);
-                    umma_commit(&h_full[x]);
+                    umma_commit(&h_full[xh]);
                 }
-                if (!ok) break;
-                umma_commit(&l_full[lb]);
-                q++;
             }
             // every MMA issued so far completes before tensor memory is freed
             umma_commit(drain);
@@ -311,68 +337,66 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
         __syncwarp();
     } else if (warp < 2 + TC_GEN_WARPS) {
         // ---------------- generators ----------------
+        // Lane l owns tile rows jj*32 + l (jj = 0..3): output cell slot
+        // l / (VB/4) and the 4 consecutive VDFs 4*(l % (VB/4)) + jj, so one
+        // 16-byte shared load gives the f values of all 4 rows.
         const int kg = warp - 2;  // k-group of this warp: pairs 8 kg .. 8 kg + 7 of a chunk
-        int Dc[NDG];
-#pragma unroll
-        for (int d = 0; d < NDG; d++) Dc[d] = D0 + d;
+        constexpr int LPC = VB / 4;                             // lanes per output cell
+        constexpr int SH = VB == 128 ? 0 : (VB == 64 ? 1 : 2);  // offsets are stored for VB = 128
+        const int dl = lane / LPC, vq = lane % LPC;
         int g = 0, q = 0;
         bool ok = true;
-        for (int b = a.b0; b < a.b1 && ok; b++) {
-            const BlockInfo bi = a.blk[b];
-            if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
-            bool valid[NDG];
-#pragma unroll
-            for (int d = 0; d < NDG; d++) {
-                const int D = Dc[d];
-                const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
-                valid[d] = D < a.Nc && Du >= bi.lo[0] && Du <= bi.hi[0] && Dv >= bi.lo[1] && Dv <= bi.hi[1] &&
-                           Dw >= bi.lo[2] && Dw <= bi.hi[2];
-            }
+        for (int it = i0; it < i1 && ok; it++) {
+            const TcItem e = a.items[it];
+            const bool valid = (e.nch >> (16 + dl)) & 1;
             const int fb = q & 1;
             if (!mbar_wait_warp(&f_full[fb], (q >> 1) & 1, a.err)) { ok = false; break; }
-            const float *f1 = fs + (size_t)(2 * fb) * NDG * cell_floats + lane;
+            // rows of cells outside the block's box read stale (in-bounds) shared
+            // memory and are zeroed below
+            const float *f1 = fs + (size_t)(2 * fb) * NDG * cell_floats + (size_t)dl * cell_floats + 4 * vq;
             const float *f2 = f1 + (size_t)NDG * cell_floats;
-            const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
-            for (int c = c0; c < c1; c++, g++) {
-                const int s = g % TC_NSTB, x = g & 1;
+            const int nch = e.nch & 0xffff;
+            for (int c = 0; c < nch; c++, g++) {
+                const int s = g % TC_NSTB, xa = g % TC_NA;
                 if (!mbar_wait_warp(&b_full[s], (g / TC_NSTB) & 1, a.err)) { ok = false; break; }
-                if (!mbar_wait_warp(&a_empty[x], ((g >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
-                const uint4 iv = *reinterpret_cast<const uint4 *>(vring + s * TC_REC + 2 * TC_TILE_B + 16 * kg);
-                const uint32_t w4[4] = {iv.x, iv.y, iv.z, iv.w};
-                int o1[8], o2[8];  // f offsets (floats) of the 8 pairs
+                if (!mbar_wait_warp(&a_empty[xa], ((g / TC_NA) & 1) ^ 1, a.err)) { ok = false; break; }
+                const uint4 *ip = reinterpret_cast<const uint4 *>(vring + s * TC_REC + 2 * TC_TILE_B + 32 * kg);
+                const uint4 i0v = ip[0], i1v = ip[1];
+                const uint32_t w8[8] = {i0v.x, i0v.y, i0v.z, i0v.w, i1v.x, i1v.y, i1v.z, i1v.w};
+                float xv[8][4];
+                float4 a1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                uint32_t prev = 0xffffffffu;
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
-                    const uint32_t wd = w4[j >> 1] >> (16 * (j & 1));
-                    o1[j] = (int)(wd & 0xffu) * VB;
-                    o2[j] = (int)((wd >> 8) & 0xffu) * VB;
-                }
-                unsigned char *ah = abuf + (2 * x) * TC_ATILE, *al = abuf + (2 * x + 1) * TC_ATILE;
-#pragma unroll
-                for (int d = 0; d < NDG; d++) {
-                    const float *p1 = f1 + d * cell_floats, *p2 = f2 + d * cell_floats;
-#pragma unroll
-                    for (int jj = 0; jj < NJ; jj++) {
-                        const int row = d * VB + jj * 32 + lane;
-                        uint32_t hi[4], lo[4];
-                        if (valid[d]) {
-                            float x8[8];
-#pragma unroll
-                            for (int j = 0; j < 8; j++) x8[j] = p1[o1[j] + jj * 32] * p2[o2[j] + jj * 32];
-#pragma unroll
-                            for (int j = 0; j < 4; j++) split2(x8[2 * j], x8[2 * j + 1], hi[j], lo[j]);
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < 4; j++) { hi[j] = 0u; lo[j] = 0u; }
-                        }
-                        // core matrix (row/8, kg): 8 rows x 16 bytes
-                        const int off = ((row >> 3) * 8 + kg) * 128 + (row & 7) * 16;
-                        *reinterpret_cast<uint4 *>(ah + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                        *reinterpret_cast<uint4 *>(al + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                    const uint32_t o1 = (w8[j] & 0xffffu) >> SH, o2 = (w8[j] >> 16) >> SH;
+                    if (o1 != prev) {  // pairs are sorted by l1: reuse the last f1 load
+                        a1 = *reinterpret_cast<const float4 *>(f1 + o1);
+                        prev = o1;
                     }
+                    const float4 a2 = *reinterpret_cast<const float4 *>(f2 + o2);
+                    const float2 p01 = fmul2(make_float2(a1.x, a1.y), make_float2(a2.x, a2.y));
+                    const float2 p23 = fmul2(make_float2(a1.z, a1.w), make_float2(a2.z, a2.w));
+                    xv[j][0] = p01.x; xv[j][1] = p01.y; xv[j][2] = p23.x; xv[j][3] = p23.y;
+                }
+                unsigned char *ah = abuf + (2 * xa) * TC_ATILE, *al = abuf + (2 * xa + 1) * TC_ATILE;
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) {
+                    const int row = jj * 32 + lane;
+                    uint32_t hi[4], lo[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) split2(xv[2 * j][jj], xv[2 * j + 1][jj], hi[j], lo[j]);
+                    if (!valid) {
+#pragma unroll
+                        for (int j = 0; j < 4; j++) { hi[j] = 0u; lo[j] = 0u; }
+                    }
+                    // core matrix (row/8, kg): 8 rows x 16 bytes
+                    const int off = ((row >> 3) * 8 + kg) * 128 + (row & 7) * 16;
+                    *reinterpret_cast<uint4 *>(ah + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                    *reinterpret_cast<uint4 *>(al + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
                 }
                 fence_async_shared();  // generic-proxy writes -> visible to the tensor core
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&a_full[x]);
+                if (lane == 0) mbar_arrive(&a_full[xa]);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&f_empty[fb]);  // this warp's reads of the f slot are done
@@ -387,40 +411,35 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
         for (int i = 0; i < 32; i++) run[i] = 0.f;
 #pragma unroll
         for (int h = 0; h < 4; h++) tmem_st16(tl + 128 + 16 * h, run);
-        int g = 0, q = 0;
+        int g = 0;
         bool ok = true;
-        for (int b = a.b0; b < a.b1 && ok; b++) {
-            const BlockInfo bi = a.blk[b];
-            if (!dgroup_meets<NDG>(bi, D0, a.Nc, a.Mv, a.Mw)) continue;
-            const int c0 = a.chunk_start[b], c1 = a.chunk_start[b + 1];
-            for (int c = c0; c < c1; c++, g++) {
-                const int x = g & 1;
-                if (!mbar_wait_warp(&h_full[x], (g >> 1) & 1, a.err)) { ok = false; break; }
+        for (int it = i0; it < i1 && ok; it++) {
+            const int nch = a.items[it].nch & 0xffff;
+            for (int c = 0; c < nch; c++, g++) {
+                const int xh = g & 1;
+                if (!mbar_wait_warp(&h_full[xh], (g >> 1) & 1, a.err)) { ok = false; break; }
                 tc_fence_after();
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    float v[16];
-                    tmem_ld16(tl + x * 32 + 16 * h, v);
+                    float vh[16], vl[16];
+                    tmem_ld16(tl + xh * 64 + 16 * h, vh);
+                    tmem_ld16(tl + xh * 64 + 32 + 16 * h, vl);
 #pragma unroll
-                    for (int i = 0; i < 16; i++) run[16 * h + i] += v[i];
+                    for (int i = 0; i < 16; i++) run[16 * h + i] += vh[i] + vl[i];
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&h_empty[x]);
+                if (lane == 0) mbar_arrive(&h_empty[xh]);
             }
             if (!ok) break;
-            const int lb = q & 1;
-            if (!mbar_wait_warp(&l_full[lb], (q >> 1) & 1, a.err)) { ok = false; break; }
-            tc_fence_after();
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                float v[16], sm[16], cm[16];
-                tmem_ld16(tl + 64 + lb * 32 + 16 * h, v);
+            for (int h = 0; h < 2; h++) {  // two-sum of the block total into (sum, correction)
+                float sm[16], cm[16];
                 tmem_ld16(tl + 128 + 16 * h, sm);
                 tmem_ld16(tl + 160 + 16 * h, cm);
 #pragma unroll
-                for (int i = 0; i < 16; i++) {  // two-sum of sum + block total
-                    const float xb = run[16 * h + i] + v[i];
+                for (int i = 0; i < 16; i++) {
+                    const float xb = run[16 * h + i];
                     const float t = sm[i] + xb, bp = t - sm[i];
                     cm[i] += (sm[i] - (t - bp)) + (xb - bp);
                     sm[i] = t;
@@ -429,13 +448,11 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
                 tmem_st16(tl + 128 + 16 * h, sm);
                 tmem_st16(tl + 160 + 16 * h, cm);
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&l_empty[lb]);
-            q++;
         }
         if (ok) {
-            const int d = r / VB, vdf = bt * VB + (r % VB);
+            // tile row r = jj*32 + l: cell slot l / (VB/4), VDF 4*(l % (VB/4)) + jj
+            const int l = r & 31, jj = r >> 5;
+            const int d = l / (VB / 4), vdf = bt * VB + 4 * (l % (VB / 4)) + jj;
             const int D = D0 + d;
             const bool mine = D < a.Nc && vdf < a.nvdf;
             const double sc = mine ? a.inv_scale[vdf] : 0.0;
@@ -464,7 +481,7 @@ __global__ void __launch_bounds__(512, 1) k_collide_tc(TcArgs a)
 
 // ----------------------------------------------------------------------------
 // chunk records: per block, ceil(count/64) records of {V hi tile, V lo tile,
-// (l1,l2) bytes}; tiles K-major without swizzle: element (p, k) at byte
+// per pair the f offsets l1*128 | l2*128 << 16}; tiles K-major without swizzle: element (p, k) at byte
 // ((p/8)*8 + k/8)*128 + (p%8)*16 + (k%8)*2
 __global__ void k_tc_build(const BlockInfo *blk, const double *rows64, int RD64, const int *chunk_start, int P,
                            int Nc, int ccell, float vscale, unsigned char *V)
@@ -483,8 +500,8 @@ __global__ void k_tc_build(const BlockInfo *blk, const double *rows64, int RD64,
             l1 = (o1 - (bi.c1 - ccell)) / Nc;
             l2 = (o2 - (bi.c2 - ccell)) / Nc;
         }
-        rec[2 * TC_TILE_B + 2 * k] = (unsigned char)l1;
-        rec[2 * TC_TILE_B + 2 * k + 1] = (unsigned char)l2;
+        // f offsets (floats) of the two factors in a 128-VDF tile slice
+        *reinterpret_cast<uint32_t *>(rec + 2 * TC_TILE_B + 4 * k) = (uint32_t)(l1 * 128) | ((uint32_t)(l2 * 128) << 16);
         for (int p = 0; p < 32; p++) {
             float x = (real && p < P) ? (float)(row[1 + p] * (double)vscale) : 0.f;
             __half h = __float2half_rn(x);
@@ -605,54 +622,89 @@ static int tc_prepare(Ctx *c)
     return DGV_OK;
 }
 
-// Row-tile order per launch: tiles (groups of NDG output cells) sorted by the
-// chunk records they consume, heaviest first, so the last wave of CTAs is
-// short.  One array of nsets x ngroups on the device, built once per NDG.
-static int tc_order(Ctx *c, int NDG, const int **d_order)
+// Work lists, built once per cells-per-tile NDG: for every launch (block
+// set) and row tile (NDG consecutive output cells), the blocks whose valid
+// box meets the tile, in block order, with the tile cells each is valid for.
+// Tiles of a launch are ordered by the chunk records they consume, heaviest
+// first, so the last wave of CTAs is short.
+struct TcLists {
+    TcItem *items = nullptr;
+    int *item_start = nullptr;  // per set: ntiles + 1 entries
+    int *tile_of = nullptr;     // per set: ntiles entries
+};
+
+static int tc_lists(Ctx *c, int NDG, TcLists *out)
 {
     Layout &L = c->lay;
-    auto it = L.tc_order.find(NDG);
-    if (it != L.tc_order.end()) { *d_order = it->second; return DGV_OK; }
+    auto it = L.tc_lists.find(NDG);
+    if (it != L.tc_lists.end()) {
+        out->items = reinterpret_cast<TcItem *>(it->second[0]);
+        out->item_start = reinterpret_cast<int *>(it->second[1]);
+        out->tile_of = reinterpret_cast<int *>(it->second[2]);
+        return DGV_OK;
+    }
     const Grid &g = c->grid;
     const int ng = (g.Nc + NDG - 1) / NDG, nsets = (int)L.tc_sets.size() - 1;
-    std::vector<int> all((size_t)nsets * ng);
+    std::vector<TcItem> items;
+    std::vector<int> start((size_t)nsets * (ng + 1)), tile_of((size_t)nsets * ng);
+    std::vector<std::vector<TcItem>> per(ng);
     std::vector<long long> work(ng);
-    std::vector<int> stamp(ng, -1);
     for (int s = 0; s < nsets; s++) {
+        for (auto &v : per) v.clear();
         std::fill(work.begin(), work.end(), 0);
         for (int b = L.tc_sets[s]; b < L.tc_sets[s + 1]; b++) {
             const BlockInfo &bi = L.h_blk[b];
             const int ch = L.tc_chunk_host[b + 1] - L.tc_chunk_host[b];
+            int last = -1;
             for (int u = bi.lo[0]; u <= bi.hi[0]; u++)
                 for (int v = bi.lo[1]; v <= bi.hi[1]; v++)
                     for (int w = bi.lo[2]; w <= bi.hi[2]; w++) {
-                        const int grp = ((u * g.d.Mv + v) * g.d.Mw + w) / NDG;
-                        if (stamp[grp] != b) { stamp[grp] = b; work[grp] += ch; }
+                        const int D = (u * g.d.Mv + v) * g.d.Mw + w, grp = D / NDG;
+                        if (grp != last) {  // cells of one tile are consecutive: same tile as the last cell or new
+                            if (per[grp].empty() || per[grp].back().chunk0 != L.tc_chunk_host[b]) {
+                                per[grp].push_back(TcItem{L.tc_chunk_host[b], ch, bi.c1, bi.c2});
+                                work[grp] += ch;
+                            }
+                            last = grp;
+                        }
+                        per[grp].back().nch |= 1 << (16 + D % NDG);
                     }
         }
-        int *o = all.data() + (size_t)s * ng;
+        int *o = tile_of.data() + (size_t)s * ng;
         std::iota(o, o + ng, 0);
         std::stable_sort(o, o + ng, [&](int x, int y) { return work[x] > work[y]; });
+        int *st = start.data() + (size_t)s * (ng + 1);
+        for (int t = 0; t < ng; t++) {
+            st[t] = (int)items.size();
+            items.insert(items.end(), per[o[t]].begin(), per[o[t]].end());
+        }
+        st[ng] = (int)items.size();
     }
-    int *d = nullptr;
-    DGV_CUDA(c, cudaMalloc(&d, sizeof(int) * all.size()));
-    DGV_CUDA(c, cudaMemcpy(d, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
-    L.tc_order[NDG] = d;
-    *d_order = d;
+    if (items.size() > (size_t)INT32_MAX) return set_err(c, DGV_EUNSUP, "tensor-core path: work list too long");
+    void *d[3] = {nullptr, nullptr, nullptr};
+    DGV_CUDA(c, cudaMalloc(&d[0], sizeof(TcItem) * std::max<size_t>(1, items.size())));
+    DGV_CUDA(c, cudaMalloc(&d[1], sizeof(int) * start.size()));
+    DGV_CUDA(c, cudaMalloc(&d[2], sizeof(int) * tile_of.size()));
+    if (!items.empty()) DGV_CUDA(c, cudaMemcpy(d[0], items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice));
+    DGV_CUDA(c, cudaMemcpy(d[1], start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
+    DGV_CUDA(c, cudaMemcpy(d[2], tile_of.data(), sizeof(int) * tile_of.size(), cudaMemcpyHostToDevice));
+    L.tc_lists[NDG] = {d[0], d[1], d[2]};
+    out->items = reinterpret_cast<TcItem *>(d[0]);
+    out->item_start = reinterpret_cast<int *>(d[1]);
+    out->tile_of = reinterpret_cast<int *>(d[2]);
     return DGV_OK;
 }
 
 template <int VB>
-static int launch_tc(Ctx *c, TcArgs &a, const int *d_order, int ng)
+static int launch_tc(Ctx *c, TcArgs &a, const TcLists &tl, int ng)
 {
-    const size_t smem = (size_t)a.off_f + 2 * (size_t)a.fslot + (2 * TC_NSTB + 20) * sizeof(uint64_t) + 16;
+    const size_t smem = (size_t)a.off_f + 2 * (size_t)a.fslot + (2 * TC_NSTB + 2 * TC_NA + 10) * sizeof(uint64_t) + 16;
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc<VB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
     const Layout &L = c->lay;
     for (size_t s = 0; s + 1 < L.tc_sets.size(); s++) {
-        a.b0 = L.tc_sets[s];
-        a.b1 = L.tc_sets[s + 1];
-        a.order = d_order + s * ng;
+        a.item_start = tl.item_start + s * (ng + 1);
+        a.tile_of = tl.tile_of + s * ng;
         k_collide_tc<VB><<<(unsigned)(a.nbt * ng), TC_THREADS, smem, c->stream>>>(a);
         DGV_CUDA(c, cudaGetLastError());
     }
@@ -680,8 +732,8 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
     if (rc) return rc;
     rc = ensure_buffer(c, &c->d_tcQ, &c->tcQ_bytes, qbytes);
     if (rc) return rc;
-    const int *d_order = nullptr;
-    rc = tc_order(c, NDG, &d_order);
+    TcLists tl;
+    rc = tc_lists(c, NDG, &tl);
     if (rc) return rc;
     float *F = reinterpret_cast<float *>(c->d_tcF);
     double *inv = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_tcF) + fbytes);
@@ -689,15 +741,15 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
     TcArgs a;
-    a.F = F; a.V = (const unsigned char *)L.tc_V; a.chunk_start = L.tc_chunk_start; a.blk = L.blk;
-    a.order = nullptr; a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
-    a.Nc = g.Nc; a.P = g.P; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
-    a.off_f = 4 * TC_ATILE + TC_NSTB * TC_REC;                 // 16-byte aligned
-    a.fslot = 2 * NDG * g.P * VB * (int)sizeof(float);         // both sides of one block
+    a.F = F; a.V = (const unsigned char *)L.tc_V; a.items = tl.items; a.item_start = nullptr; a.tile_of = nullptr;
+    a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
+    a.Nc = g.Nc; a.P = g.P; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
+    a.off_f = 2 * TC_NA * TC_ATILE + TC_NSTB * TC_REC;  // 16-byte aligned
+    a.fslot = 2 * NDG * g.P * VB * (int)sizeof(float);  // both sides of one block
     switch (VB) {
-    case 128: rc = launch_tc<128>(c, a, d_order, ng); break;
-    case 64: rc = launch_tc<64>(c, a, d_order, ng); break;
-    default: rc = launch_tc<32>(c, a, d_order, ng); break;
+    case 128: rc = launch_tc<128>(c, a, tl, ng); break;
+    case 64: rc = launch_tc<64>(c, a, tl, ng); break;
+    default: rc = launch_tc<32>(c, a, tl, ng); break;
     }
     if (rc) return rc;
     long long tot = (long long)nvdf * g.N;

@@ -71,7 +71,8 @@ struct Layout {
     double tc_vscale = 1.0;
     std::vector<int> tc_chunk_host;
     std::vector<int> tc_sets;
-    std::map<int, int *> tc_order;   // device row-tile orders, keyed by cells per tile
+    // device work lists {items, item starts, tile order}, keyed by cells per tile
+    std::map<int, std::vector<void *>> tc_lists;
 };
 void free_layout(Layout &L);
 
