@@ -5,9 +5,11 @@ velocity distributions on the grid s=3 nodes x M=9 cells per axis on
 [-7,7]^3 (N = 19683 nodes), A-arrays = seeded synthetic records with the
 reference's index structure (generated on the device), VDFs = seeded mixtures
 of 1-4 Maxwellians (weights ~ Dirichlet(1), bulk velocities ~ U[-2,2]^3,
-temperatures ~ U[0.5,2], density 1).  The headline arm is the batched FP32
-(compensated) path with the FP64 conservation projection; the plain FP64 path
-on the same batch is timed beside it and its error against it stated.
+temperatures ~ U[0.5,2], density 1).  The headline arm is the batched
+tensor-core path (split-fp16 operands, compensated accumulation) with the FP64
+conservation projection; the plain FP64 path is timed beside it on the first
+32 VDFs of the same batch, and the error of the tensor-core path against it
+is stated.
 
 Multi-GPU: one process per GPU (torchrun); each rank evaluates its own 256
 VDFs (weak scaling, no data-path collective); time = max over ranks.
@@ -187,6 +189,16 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def load_profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/k_collide_tc_27cubed_b256.json), or None."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "k_collide_tc_27cubed_b256.json")))
+        return float(d["dram_bytes_per_launch"]), d.get("note", "")
+    except Exception:
+        return None, ""
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -202,60 +214,75 @@ def run_ours(args, world, rank, local):
     N = solver.N
     fb = mixture_batch(solver.nodes_u, solver.nodes_v, solver.nodes_w, solver.nodes_gwts, BATCH, 1000 + rank)
     f_dev = torch.tensor(fb, dtype=torch.float64, device=f"cuda:{local}")
-    q32 = torch.empty_like(f_dev)
-    q64 = torch.empty_like(f_dev)
+    qtc = torch.empty_like(f_dev)
     solver.set_projection(True)
 
-    def step32():
-        solver.EvalCollisionPeriodicAPlus_DGV(f_dev, q32, precision="f32c")
+    def step():
+        solver.EvalCollisionPeriodicAPlus_DGV(f_dev, qtc, precision="tc")
 
+    t = time.perf_counter()
     with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step32()
+        step()  # first call builds the tensor-core layout and work lists
         torch.cuda.synchronize()
+    t_prep = time.perf_counter() - t
+    solver.set_kernel_timing(True)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup - 1):
+            step()
+        torch.cuda.synchronize()
+        solver.kernel_stats(reset=True)
         barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
             e0.record(stream)
             for _ in range(args.steps):
-                step32()
+                step()
             e1.record(stream)
             torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         barrier(world)
         torch.cuda.synchronize()
+    kst = solver.kernel_stats(reset=True)
+    solver.set_kernel_timing(False)
     ms_max = max_over_ranks(ms, world)
     value = world * BATCH * args.steps / (ms_max / 1000.0)
 
-    # plain FP64 path on the same batch (and the error of the FP32 path against it)
+    # plain FP64 path on the first NB64 VDFs of the batch (its throughput per
+    # VDF does not depend on the batch size) and the error of the
+    # tensor-core path against it; both with the FP64 conservation projection
+    NB64 = min(BATCH, args.f64_vdfs)
+    f64_in = f_dev[:NB64].contiguous()
+    q64 = torch.empty_like(f64_in)
     with torch.cuda.stream(stream):
-        solver.EvalCollisionPeriodicAPlus_DGV(f_dev[:8].contiguous(), q64[:8], precision="f64")
+        solver.EvalCollisionPeriodicAPlus_DGV(f64_in, q64, precision="f64")  # warm-up (chunk choice, buffers)
         torch.cuda.synchronize()
         e0.record(stream)
-        solver.EvalCollisionPeriodicAPlus_DGV(f_dev, q64, precision="f64")
+        solver.EvalCollisionPeriodicAPlus_DGV(f64_in, q64, precision="f64")
         e1.record(stream)
         torch.cuda.synchronize()
     ms64 = max_over_ranks(e0.elapsed_time(e1), world)
-    value64 = world * BATCH / (ms64 / 1000.0)
-    q32h, q64h = q32.cpu().numpy(), q64.cpu().numpy()
-    errs = np.linalg.norm(q32h - q64h, axis=1) / np.linalg.norm(q64h, axis=1)
+    value64 = world * NB64 / (ms64 / 1000.0)
+    qtch, q64h = qtc[:NB64].cpu().numpy(), q64.cpu().numpy()
+    errs = np.linalg.norm(qtch - q64h, axis=1) / np.linalg.norm(q64h, axis=1)
+    merrs = np.abs(qtch - q64h).max(axis=1) / np.abs(q64h).max(axis=1)
     psi = [np.ones(N), solver.nodes_u, solver.nodes_v, solver.nodes_w,
            solver.nodes_u ** 2 + solver.nodes_v ** 2 + solver.nodes_w ** 2]
+    qall = qtc.cpu().numpy()
     cons = max(abs(np.sum(solver.nodes_gwts * p_ * q)) / np.sum(np.abs(solver.nodes_gwts * p_ * q))
-               for q in q32h[:8] for p_ in psi)
+               for q in qall for p_ in psi)
 
     # end to end through the C-ABI with host buffers (pinned): H2D + compute + D2H per step
     f_host = torch.tensor(fb, dtype=torch.float64).pin_memory()
     q_host = torch.empty_like(f_host).pin_memory()
     fh, qh = f_host.numpy(), q_host.numpy()
-    solver.EvalCollisionPeriodicAPlus_DGV(fh, qh, precision="f32c")
+    solver.EvalCollisionPeriodicAPlus_DGV(fh, qh, precision="tc")
     barrier(world)
     with torch.cuda.stream(stream):
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
-            solver.EvalCollisionPeriodicAPlus_DGV(fh, qh, precision="f32c")
+            solver.EvalCollisionPeriodicAPlus_DGV(fh, qh, precision="tc")
         e1.record(stream)
         torch.cuda.synchronize()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1), world)
@@ -263,41 +290,47 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return
-    peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        hbm_peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+        tc_peak, peak_src = float(peaks["bf16_tflops_sustained"]), "measured (bf16 sustained)"
     except Exception:
-        hbm_peak, peak_src = 6650.0, "fallback"
-    ms_step = ms / args.steps
-    rows32_bytes = info["pairs"] * ((2 + solver.P + 3) // 4 * 4) * 4
-    alg_bytes = rows32_bytes + 2 * N * BATCH * 8
-    achieved = alg_bytes / (ms_step / 1000.0) / 1e9
-    launches_per_step = 4  # collide, chunk reduce, projection moments, projection apply
+        tc_peak, peak_src = 1400.0, "fallback (bf16 sustained)"
+    # algorithmic work: one record-shift = A * f(a) * f(b) accumulated = 3 FLOPs
+    alg_flop_eval = 3.0 * info["record_shifts"]
+    k_ms_launch = kst["ms"] / max(kst["launches"], 1)
+    alg_flop_launch = alg_flop_eval * BATCH * args.steps / max(kst["launches"], 1)
+    achieved = alg_flop_launch / (k_ms_launch / 1000.0) / 1e12
+    traffic, tnote = load_profile_traffic()
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16 hi+lo split products, f32 accumulate, f64 sums",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": "s=3,M=9,L=7", "batch_per_gpu": BATCH, "global_batch": BATCH * world,
-                   "precision": "f32c (FP32 products, two-sum accumulation) + FP64 conservation projection",
+                   "precision": "tensor cores (tcgen05): split-fp16 operands, compensated FP32/FP64 accumulation, "
+                                "FP64 conservation projection",
                    "A": f"seeded synthetic records, reference index structure: {info['records']} records, "
                         f"{info['pairs']} pairs, {info['blocks']} cell-pair blocks",
                    "record_shifts_per_eval": info["record_shifts"],
-                   "l2": "inputs larger than L2 (A rows {:.1f} GB per step)".format(rows32_bytes / 1e9),
+                   "l2": "inputs larger than L2: A chunk records (~8 GB) are streamed from HBM every step",
                    "parallelism": f"replicas over VDFs, dp{world}"},
-        "f64_plain_evals_per_s": value64, "f32c_over_f64": value / value64,
-        "err_f32c_vs_f64_max": float(errs.max()), "conservation_rel_max": float(cons),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
-                     "kernel": "k_collide_f32c<27>",
-                     "note": "algorithmic bytes = FP32 A rows read once per launch + f in + Q out; the kernel is "
-                             "bound by shared-memory gathers and FMA issue, not HBM"},
+        "f64_plain_evals_per_s": value64, "f64_timed_vdfs": NB64, "tc_over_f64": value / value64,
+        "err_tc_vs_f64_norm_max": float(errs.max()), "err_tc_vs_f64_maxabs_rel_max": float(merrs.max()),
+        "conservation_rel_max": float(cons),
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": achieved / tc_peak, "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "k_collide_tc<128>", "launches_per_step": kst["launches"] / args.steps,
+                     "kernel_ms_per_launch": k_ms_launch,
+                     "alg_flop_per_launch": alg_flop_launch,
+                     "note": "algorithmic FLOPs = 3 per record-shift (A*f*f + add) x VDFs; the kernel issues "
+                             "3 fp16 products per term (hi*hi, hi*lo, lo*hi) on M=128 x N<=64 tiles. "
+                             "traffic = ncu dram read+write bytes per launch. " + tnote},
         "cpu_baseline": None,
         "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(BATCH * N * 8),
                 "d2h_bytes_per_step": int(BATCH * N * 8)},
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": int(kst["all_launches"]),
         "clocks": clk.summary(),
-        "setup_s": {"synthetic_A": t_gen},
+        "setup_s": {"synthetic_A": t_gen, "tensor_core_layout_and_lists": t_prep},
     }
     if world == 1 and not args.no_cpu_baseline:
         cb, _ = cpu_baseline(seconds_target=args.ref_seconds)
@@ -306,18 +339,20 @@ def run_ours(args, world, rank, local):
 
 
 def run_profile_case(case: str):
-    """Small case for profiler captures on the 21^3 grid (s=3, M=7, [-6,6]^3;
-    A rows ~5.6 GB in total): one VDF with a fixed chunk count (no tuning
-    launches) for the CUDA-core kernels, a batch of 256 VDFs for the
-    tensor-core kernel (one launch per block set); one warm-up evaluation,
-    then one evaluation to capture."""
+    """Cases for profiler captures.  "<prec>_21": the 21^3 grid (s=3, M=7,
+    [-6,6]^3; A rows ~5.6 GB in total) -- one VDF with a fixed chunk count (no
+    tuning launches) for the CUDA-core kernels, a batch of 256 VDFs for the
+    tensor-core kernel (one launch per block set).  "tc_27": the benchmark
+    workload itself (27^3 x 256 VDFs), for single-pass counters only.  Two
+    evaluations each: a warm-up, then the one to capture."""
     import torch
 
     import dgv0d3v_direct_collision_b200 as dgv
-    prec = case.split("_")[0]
-    s = dgv.DGVSolver(3, 7, 6.0)
+    prec, grid = case.split("_")
+    s = dgv.DGVSolver(S, M, L) if grid == "27" else dgv.DGVSolver(3, 7, 6.0)
     s.generate_synthetic_A(seed=SEED_A, support=1)
-    s.set_nchunks(296)
+    if prec != "tc":
+        s.set_nchunks(296)
     nb = BATCH if prec == "tc" else 1
     fb = mixture_batch(s.nodes_u, s.nodes_v, s.nodes_w, s.nodes_gwts, nb, 3)
     f = torch.tensor(fb if nb > 1 else fb[0], dtype=torch.float64, device="cuda")
@@ -336,7 +371,7 @@ def run_profile_case(case: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21"], default=None,
+    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21", "tc_27"], default=None,
                     help="small single-VDF case for profiler captures (no JSON bench line)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -344,6 +379,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--f64-vdfs", type=int, default=32,
+                    help="VDFs of the batch the plain FP64 arm is timed on")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libdgv_b200.so")
 
 DGV_OK, DGV_EINVAL, DGV_ERANGE, DGV_ECUDA, DGV_ETIMEOUT, DGV_ENOMEM, DGV_ESTATE, DGV_EUNSUP = range(8)
 DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC = 0, 1, 2
-DGV_OPT_PROJECT, DGV_OPT_NCHUNKS = 1, 2
+DGV_OPT_PROJECT, DGV_OPT_NCHUNKS, DGV_OPT_KTIMING = 1, 2, 3
 
 STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4: "DGV_ETIMEOUT",
                 5: "DGV_ENOMEM", 6: "DGV_ESTATE", 7: "DGV_EUNSUP"}
@@ -21,7 +21,7 @@ STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4
 # every entry point include/dgv_b200.h declares
 EXPORTS = [
     "dgv_ctx_create", "dgv_ctx_destroy", "dgv_last_error", "dgv_set_stream", "dgv_set_async",
-    "dgv_set_option", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
+    "dgv_set_option", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_spatial_oper",
     "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
     "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
@@ -62,6 +62,7 @@ def load() -> C.CDLL:
         "dgv_set_stream": [vp, vp],
         "dgv_set_async": [vp, C.c_int],
         "dgv_set_option": [vp, C.c_int, i64],
+        "dgv_kernel_stats": [vp, C.POINTER(dbl), C.POINTER(i64), C.POINTER(i64), C.c_int],
         "dgv_grid_info": [vp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)],
         "dgv_nodes": [vp, vp, vp, vp, vp],
         "dgv_load_A": [vp, i64, vp, vp, vp, vp, C.c_int],

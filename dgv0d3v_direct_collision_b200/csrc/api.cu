@@ -106,10 +106,51 @@ static int gram_inverse(Ctx *c)
     return DGV_OK;
 }
 
+KTimer::KTimer(Ctx *ctx) : c(ctx)
+{
+    if (!c->ktiming) return;
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return;
+    if (!c->kt_pool.empty()) {
+        ev = c->kt_pool.back();
+        c->kt_pool.pop_back();
+    } else if (cudaEventCreate(&ev.first) != cudaSuccess || cudaEventCreate(&ev.second) != cudaSuccess) {
+        return;
+    }
+    on = cudaEventRecord(ev.first, c->stream) == cudaSuccess;
+}
+
+void KTimer::stop(long long nlaunch)
+{
+    if (!on) return;
+    if (cudaEventRecord(ev.second, c->stream) == cudaSuccess) {
+        c->kt_pending.push_back(ev);
+        c->kt_launches += nlaunch;
+    }
+    on = false;
+}
+
+void count_launches(Ctx *c, long long n)
+{
+    c->kt_all += n;
+}
+
+void free_ktimers(Ctx *c)
+{
+    for (auto *v : {&c->kt_pending, &c->kt_pool})
+        for (auto &pr : *v) {
+            if (pr.first) cudaEventDestroy(pr.first);
+            if (pr.second) cudaEventDestroy(pr.second);
+        }
+    c->kt_pending.clear();
+    c->kt_pool.clear();
+}
+
 static void destroy_ctx(Ctx *c)
 {
     cudaSetDevice(c->device);
     release_graphs(c);
+    free_ktimers(c);
     free_layout(c->lay);
     double *bufs[] = {c->d_nu, c->d_nv, c->d_nw, c->d_nwt, c->d_partial, c->d_in, c->d_out, c->d_red, c->d_fm,
                       c->d_tcF, c->d_tcQ};
@@ -261,8 +302,33 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
         if (value < 0 || value > 65535) return set_err(&ctx->c, DGV_EINVAL, "nchunks out of range");
         ctx->c.nchunks_opt = (int)value;
         return DGV_OK;
+    case DGV_OPT_KTIMING: ctx->c.ktiming = value != 0; return DGV_OK;
     default: return set_err(&ctx->c, DGV_EINVAL, "unknown option");
     }
+}
+
+int dgv_kernel_stats(dgv_ctx *ctx, double *ms, int64_t *launches, int64_t *all_launches, int reset)
+{
+    CTX_CHECK(ctx);
+    Ctx *c = &ctx->c;
+    DGV_CUDA(c, cudaSetDevice(c->device));
+    for (auto &pr : c->kt_pending) {
+        float t = 0.f;
+        DGV_CUDA(c, cudaEventSynchronize(pr.second));
+        DGV_CUDA(c, cudaEventElapsedTime(&t, pr.first, pr.second));
+        c->kt_ms += t;
+        c->kt_pool.push_back(pr);
+    }
+    c->kt_pending.clear();
+    if (ms) *ms = c->kt_ms;
+    if (launches) *launches = c->kt_launches;
+    if (all_launches) *all_launches = c->kt_all;
+    if (reset) {
+        c->kt_ms = 0.0;
+        c->kt_launches = 0;
+        c->kt_all = 0;
+    }
+    return DGV_OK;
 }
 
 int dgv_grid_info(const dgv_ctx *ctx, int64_t *N, int32_t *P, int32_t *Nc, int32_t *ccell)

@@ -332,18 +332,22 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     // VDF fastest: the CTAs resident at one time work on the same chunk of
     // rows for different VDFs, so each row is fetched from HBM once and then
     // served from L2
+    KTimer kt(c);
     fn<<<dim3(nvdf, sh.slices, nchunks), sh.threads, sh.smem, c->stream>>>(a);
+    kt.stop(1);
     DGV_CUDA(c, cudaGetLastError());
     long long tot = (long long)nvdf * g.N;
     k_reduce_chunks<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_partial, c->d_nwt, d_q, nchunks, g.P,
                                                                              g.Nc, g.N, nvdf, scale);
     DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 2);
     return DGV_OK;
 }
 
-// Chunk count.  Many VDFs: the smallest count whose last wave of CTAs is at
-// least 90% full (one CTA per SM: the shared copy of f takes most of it).
-// Few VDFs: measured -- each candidate is timed once and the fastest kept.
+// Chunk count.  Batches that fill at least a quarter of the SMs: the smallest
+// count whose last wave of CTAs is at least 90% full (one CTA per SM: the
+// shared copy of f takes most of it).  Smaller batches: measured -- each
+// candidate is timed once and the fastest kept.
 static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *d_q, int nvdf, int precision)
 {
     if (c->nchunks_opt > 0) return c->nchunks_opt;
@@ -354,7 +358,7 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
     long long units = (long long)nvdf * sh.slices;
-    if (units >= 2LL * nsm) {
+    if (units * 4 >= nsm) {
         for (int k = 1; k <= 8; k++) {
             long long ctas = units * k;
             long long waves = (ctas + nsm - 1) / nsm;

@@ -48,7 +48,7 @@ constexpr int TC_TILE_B = 32 * TC_KCH * 2;          // one 32 x 64 fp16 tile (4 
 constexpr int TC_REC = 2 * TC_TILE_B + TC_KCH * 4;  // hi tile, lo tile, f offsets of the pairs
 constexpr int TC_ROWS = 128;
 constexpr int TC_NSTB = 4;                          // V ring stages
-constexpr int TC_NA = 3;                            // A tile stages
+constexpr int TC_NA = 4;                            // A tile stages
 constexpr int TC_ATILE = TC_ROWS * TC_KCH * 2;      // 128 x 64 fp16 (16 KiB)
 constexpr int TC_THREADS = 448;
 constexpr int TC_GEN_WARPS = 8;
@@ -702,12 +702,15 @@ static int launch_tc(Ctx *c, TcArgs &a, const TcLists &tl, int ng)
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc<VB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
     const Layout &L = c->lay;
+    KTimer kt(c);
     for (size_t s = 0; s + 1 < L.tc_sets.size(); s++) {
         a.item_start = tl.item_start + s * (ng + 1);
         a.tile_of = tl.tile_of + s * ng;
         k_collide_tc<VB><<<(unsigned)(a.nbt * ng), TC_THREADS, smem, c->stream>>>(a);
         DGV_CUDA(c, cudaGetLastError());
     }
+    kt.stop((long long)L.tc_sets.size() - 1);
+    count_launches(c, (long long)L.tc_sets.size() - 1);
     return DGV_OK;
 }
 
@@ -755,6 +758,7 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
     long long tot = (long long)nvdf * g.N;
     k_tc_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, c->d_nwt, d_q, g.N, nvdf, NV, scale);
     DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 2);  // k_tc_fprep, k_tc_final
     if (c->project) return project_device(c, d_q, nvdf);
     return DGV_OK;
 }

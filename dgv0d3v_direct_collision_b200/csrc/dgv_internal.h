@@ -110,7 +110,25 @@ struct Ctx {
     int *h_err = nullptr, *d_err = nullptr;
     // autotuned chunk counts keyed by (precision, nvdf bucket)
     std::map<long long, int> tuned;
+    // kernel timing (DGV_OPT_KTIMING): event pairs around the collision
+    // kernel's launches, summed on request; launch counters
+    bool ktiming = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
+    long long kt_launches = 0, kt_all = 0;
+    double kt_ms = 0.0;
 };
+
+// Brackets the launches of the collision kernel on the context stream with
+// CUDA events when kernel timing is on (not while the stream is captured).
+struct KTimer {
+    Ctx *c;
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    bool on = false;
+    explicit KTimer(Ctx *ctx);
+    void stop(long long nlaunch);
+};
+void count_launches(Ctx *c, long long n);
+void free_ktimers(Ctx *c);
 
 // error helpers
 int set_err(Ctx *c, int code, const std::string &msg);

@@ -97,6 +97,7 @@ int project_device(Ctx *c, double *d_q, int nvdf)
     std::memcpy(gr.inv, c->gram_inv, sizeof(gr.inv));
     k_project_apply<<<dim3(64, nvdf), 256, 0, c->stream>>>(d_q, c->d_nu, c->d_nv, c->d_nw, g.N, c->d_red, gr);
     DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 2);
     return DGV_OK;
 }
 

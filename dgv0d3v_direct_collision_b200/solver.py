@@ -27,7 +27,8 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC, DGV_OPT_PROJECT, DGV_OPT_NCHUNKS
+from ._lib import (DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC, DGV_OPT_PROJECT,
+                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING)
 
 PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C, "tc": DGV_PREC_TC}
 
@@ -122,6 +123,18 @@ class DGVSolver:
 
     def set_nchunks(self, n: int):
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_NCHUNKS, int(n)))
+
+    def set_kernel_timing(self, on: bool):
+        """Time the collision kernel's launches with CUDA events on the
+        context stream (read back with kernel_stats)."""
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_KTIMING, int(on)))
+
+    def kernel_stats(self, reset: bool = True):
+        """(device ms, launches) of the collision kernel and the number of
+        this library's kernel launches, summed since the last reset."""
+        ms, nl, na = C.c_double(), C.c_int64(), C.c_int64()
+        self._check(self._lib.dgv_kernel_stats(self._h, C.byref(ms), C.byref(nl), C.byref(na), int(reset)))
+        return {"ms": ms.value, "launches": nl.value, "all_launches": na.value}
 
     # -- A-arrays -------------------------------------------------------------
     def load_A(self, capphi, A, xi, xi1, one_based: bool = True):

@@ -52,6 +52,8 @@ extern "C" {
 /* options for dgv_set_option */
 #define DGV_OPT_PROJECT 1  /* 1: apply the FP64 conservation projection to Q  */
 #define DGV_OPT_NCHUNKS 2  /* work chunks per VDF (0 = autotune)             */
+#define DGV_OPT_KTIMING 3  /* 1: time the collision kernel with CUDA events   */
+                           /* on the context stream (read: dgv_kernel_stats)  */
 
 typedef struct dgv_ctx dgv_ctx;
 
@@ -78,6 +80,12 @@ int dgv_set_stream(dgv_ctx *ctx, void *stream);
 /* 1: device-pointer calls return without synchronising the stream */
 int dgv_set_async(dgv_ctx *ctx, int async_flag);
 int dgv_set_option(dgv_ctx *ctx, int option, int64_t value);
+/* No counterpart in the reference (measurement hook): summed device time in
+ * ms and launch count of the collision kernel (k_collide_tc / k_collide_pipe)
+ * over the calls made since the last reset while DGV_OPT_KTIMING was on,
+ * and the number of kernels of this library those calls launched.
+ * Synchronises on the recorded events; reset != 0 clears the sums. */
+int dgv_kernel_stats(dgv_ctx *ctx, double *ms, int64_t *launches, int64_t *all_launches, int reset);
 /* N, P = su*sv*sw, number of cells, canonical cell (0-based) */
 int dgv_grid_info(const dgv_ctx *ctx, int64_t *N, int32_t *P, int32_t *Nc, int32_t *ccell);
 /* host copies of nodes_u/_v/_w/_gwts (miscset.f90:1112-1183); any may be NULL */
