@@ -166,23 +166,32 @@ static void destroy_ctx(Ctx *c)
 
 // Stage an input array: device pointers pass through, host arrays are copied
 // into the context's input buffer at offset `slot` (in doubles).
+// Grows the input staging buffer to `need_doubles`, keeping its contents.
+// Growth moves the buffer: pointers handed out by stage_in before it are
+// invalid afterwards, so calls that stage several inputs reserve the total
+// first.
+static int reserve_in(Ctx *c, size_t need_doubles)
+{
+    const size_t need = need_doubles * sizeof(double);
+    if (c->in_bytes >= need) return DGV_OK;
+    release_graphs(c);  // the move invalidates captured graphs
+    double *nb = nullptr;
+    DGV_CUDA(c, cudaMalloc(&nb, need));
+    if (c->d_in) {
+        DGV_CUDA(c, cudaMemcpyAsync(nb, c->d_in, c->in_bytes, cudaMemcpyDeviceToDevice, c->stream));
+        DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->d_in);
+    }
+    c->d_in = nb;
+    c->in_bytes = need;
+    return DGV_OK;
+}
+
 static int stage_in(Ctx *c, const double *p, size_t n, size_t slot, const double **d)
 {
     if (is_device_ptr(p)) { *d = p; return DGV_OK; }
-    size_t need = (slot + n) * sizeof(double);
-    if (c->in_bytes < need) {
-        // grow keeping earlier slots (the move invalidates captured graphs)
-        release_graphs(c);
-        double *nb = nullptr;
-        DGV_CUDA(c, cudaMalloc(&nb, need));
-        if (c->d_in) {
-            DGV_CUDA(c, cudaMemcpyAsync(nb, c->d_in, c->in_bytes, cudaMemcpyDeviceToDevice, c->stream));
-            DGV_CUDA(c, cudaStreamSynchronize(c->stream));
-            cudaFree(c->d_in);
-        }
-        c->d_in = nb;
-        c->in_bytes = need;
-    }
+    int rc = reserve_in(c, slot + n);
+    if (rc) return rc;
     DGV_CUDA(c, cudaMemcpyAsync(c->d_in + slot, p, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     *d = c->d_in + slot;
     return DGV_OK;
@@ -537,6 +546,7 @@ int dgv_jvp(dgv_ctx *ctx, const double *f, const double *df, double *q, int prec
     const double *d1, *d2;
     double *dq;
     bool host = false;
+    TRY(reserve_in(c, 2 * n));  // both inputs staged: no move between them
     TRY(stage_in(c, f, n, 0, &d1));
     TRY(stage_in(c, df, n, n, &d2));
     TRY(out_ptr(c, q, n, &dq, &host));
@@ -553,6 +563,7 @@ int dgv_vjp(dgv_ctx *ctx, const double *f, const double *v, double *g, int preci
     const double *d1, *d2;
     double *dg;
     bool host = false;
+    TRY(reserve_in(c, 2 * n));  // both inputs staged: no move between them
     TRY(stage_in(c, f, n, 0, &d1));
     TRY(stage_in(c, v, n, n, &d2));
     TRY(out_ptr(c, g, n, &dg, &host));

@@ -345,7 +345,8 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
 }
 
 // Chunk count.  Batches that fill at least a quarter of the SMs: the smallest
-// count whose last wave of CTAs is at least 90% full (one CTA per SM: the
+// count giving at least 8 waves of CTAs (work per chunk varies; more, smaller
+// CTAs balance it) whose last wave is at least 90% full (one CTA per SM: the
 // shared copy of f takes most of it).  Smaller batches: measured -- each
 // candidate is timed once and the fastest kept.
 static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *d_q, int nvdf, int precision)
@@ -359,12 +360,12 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
     long long units = (long long)nvdf * sh.slices;
     if (units * 4 >= nsm) {
-        for (int k = 1; k <= 8; k++) {
+        for (int k = 1; k <= 64; k++) {
             long long ctas = units * k;
             long long waves = (ctas + nsm - 1) / nsm;
-            if ((double)ctas / (double)(waves * nsm) >= 0.9) return k;
+            if (waves >= 8 && (double)ctas / (double)(waves * nsm) >= 0.9) return k;
         }
-        return 8;
+        return 64;
     }
     long long key = ((long long)precision << 40) ^ ((long long)(d_f2 != nullptr) << 39) ^ nvdf;
     auto it = c->tuned.find(key);

@@ -131,6 +131,21 @@ def test_vjp_vs_oracle_and_fd(gsolver, golden):
     assert abs(g @ d - fd) <= 1e-8 * max(1.0, abs(fd))
 
 
+def test_two_input_calls_first_on_a_fresh_context(dgv, golden):
+    """VJP and JVP stage two host arrays; as the first call on a new context
+    the staging buffer grows while they are staged."""
+    o = golden_oracle(golden)
+    rng = np.random.default_rng(11)
+    f, v = golden["f0"], rng.standard_normal(o.N)
+    for which in ("vjp", "jvp"):
+        s = dgv.DGVSolver(int(golden["s"]), int(golden["M"]), float(golden["L"]), kappa=float(golden["kappa"]))
+        s.load_A(golden["capphi"], golden["A"], golden["A_xi"], golden["A_xi1"], one_based=True)
+        if which == "vjp":
+            assert rel_err(s.vjp(f, v), o.vjp(f, v)) < TOL64
+        else:
+            assert rel_err(s.jvp(f, v), o.mixed_terms(f, v)) < TOL64
+
+
 def test_vjp_equals_linearized_operator_at_maxwellian(gsolver, golden):
     """J^T v at fm equals 2 fmA v, the reference's linearized operator
     (collision_mod.f90:448-449, 357), within 1e-8."""
