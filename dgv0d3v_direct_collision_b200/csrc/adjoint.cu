@@ -9,7 +9,11 @@
 // keeps its P cotangent weights c_(D,p) in registers; for every pair it forms
 // vA = sum_p A_p c_p (P multiply-adds, the forward's cost) and scatters
 // vA*f(b) to g(a) and vA*f(a) to g(b) with FP64 atomic adds (so the summation
-// order, and the last bits of g, vary from run to run).
+// order, and the last bits of g, vary from run to run).  The scatter goes to a
+// local-major copy g_lm[l*Nc + cell] -- the layout of the shared copy of f,
+// so its indices are the gather offsets o1+D, o2+D -- where the 32 lanes of
+// a warp (32 consecutive cells) hit 256 contiguous bytes instead of 32 lines
+// P doubles apart; k_lm_to_nodes writes g in node order afterwards.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -103,16 +107,22 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
                 double vA = 0.0;
 #pragma unroll
                 for (int j = 0; j < PV; j++) vA = fma(rv[1 + j], cw[j], vA);
-                const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
-                const long long i1 = (long long)(q1 - l1 * a.Nc) * PV + l1;
-                const long long i2 = (long long)(q2 - l2 * a.Nc) * PV + l2;
-                atomicAdd(a.g + i1, vA * f_s[q2]);
-                atomicAdd(a.g + i2, vA * f_s[q1]);
+                atomicAdd(a.g + q1, vA * f_s[q2]);
+                atomicAdd(a.g + q2, vA * f_s[q1]);
             }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }
+}
+
+// g[cell*P + l] = g_lm[l*Nc + cell]
+__global__ void k_lm_to_nodes(const double *g_lm, double *g, long long N, int Nc, int P)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int cell = (int)(i / P), l = (int)(i - (long long)cell * P);
+    g[i] = g_lm[(size_t)l * Nc + cell];
 }
 
 typedef void (*VjpFn)(VjpArgs);
@@ -154,12 +164,17 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     if (rc) return rc;
     rc = ensure_errflag(c);
     if (rc) return rc;
-    DGV_CUDA(c, cudaMemsetAsync(d_g, 0, sizeof(double) * (size_t)g.N, c->stream));
-    a.f = d_f; a.v = d_v; a.w = c->d_nwt; a.g = d_g; a.blk = L.blk; a.rows = (const char *)L.rows64;
+    rc = ensure_buffer(c, &c->d_glm, &c->glm_bytes, sizeof(double) * (size_t)g.N);
+    if (rc) return rc;
+    DGV_CUDA(c, cudaMemsetAsync(c->d_glm, 0, sizeof(double) * (size_t)g.N, c->stream));
+    a.f = d_f; a.v = d_v; a.w = c->d_nwt; a.g = c->d_glm; a.blk = L.blk; a.rows = (const char *)L.rows64;
     a.bounds = d_bounds; a.err = c->d_err; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.dcta = dcta;
     a.rowb = rowb; a.nst = nst; a.sp = sp;
     fn<<<dim3(1, slices, nchunks), 32 + dcta, smem, c->stream>>>(a);
     DGV_CUDA(c, cudaGetLastError());
+    k_lm_to_nodes<<<(unsigned)((g.N + 255) / 256), 256, 0, c->stream>>>(c->d_glm, d_g, g.N, g.Nc, g.P);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 2);
     return DGV_OK;
 }
 

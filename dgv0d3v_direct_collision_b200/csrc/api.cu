@@ -153,7 +153,7 @@ static void destroy_ctx(Ctx *c)
     free_ktimers(c);
     free_layout(c->lay);
     double *bufs[] = {c->d_nu, c->d_nv, c->d_nw, c->d_nwt, c->d_partial, c->d_in, c->d_out, c->d_red, c->d_fm,
-                      c->d_tcF, c->d_tcQ};
+                      c->d_tcF, c->d_tcQ, c->d_glm};
     for (double *p : bufs)
         if (p) cudaFree(p);
     for (double *p : c->d_tmp)

@@ -100,6 +100,9 @@ struct Ctx {
     // tensor-core path: scaled fp32 copy of f (+ per-VDF scales), FP64 sums
     double *d_tcF = nullptr, *d_tcQ = nullptr;
     size_t tcF_bytes = 0, tcQ_bytes = 0;
+    // VJP: local-major accumulator g_lm[l*Nc + cell]
+    double *d_glm = nullptr;
+    size_t glm_bytes = 0;
     // Adams-Bashforth history: right sides frhs1..frhs5 (newest first)
     double *d_hist[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     int ab_order = 0;
