@@ -81,6 +81,8 @@ class DGVSolver:
         self.precision = precision
         self.rkmts = rkmts
         self.device = device
+        self.kappa = float(kappa)
+        self.projection = False
 
     # -- plumbing ------------------------------------------------------------
     def _check(self, rc: int):
@@ -120,6 +122,7 @@ class DGVSolver:
 
     def set_projection(self, on: bool):
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_PROJECT, int(on)))
+        self.projection = bool(on)
 
     def set_nchunks(self, n: int):
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_NCHUNKS, int(n)))
