@@ -420,6 +420,25 @@ int dgv_collide_batched(dgv_ctx *ctx, int32_t nb, const double *f, double *q, in
     return finish(c, q, dq, n, host);
 }
 
+int dgv_collide_cells(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int32_t cell0, int32_t cell1,
+                      int precision)
+{
+    CTX_CHECK(ctx);
+    Ctx *c = &ctx->c;
+    if (nb < 1 || !f || !q) return set_err(c, DGV_EINVAL, "collide_cells: need nb >= 1 and non-NULL arrays");
+    if (cell0 < 0 || cell1 > c->grid.Nc || cell0 >= cell1)
+        return set_err(c, DGV_ERANGE, "collide_cells: cell range outside [0, Nc) or empty");
+    size_t n = (size_t)nb * (size_t)c->grid.N;
+    size_t nout = (size_t)nb * (size_t)(cell1 - cell0) * (size_t)c->grid.P;
+    const double *df;
+    double *dq;
+    bool host = false;
+    TRY(stage_in(c, f, n, 0, &df));
+    TRY(out_ptr(c, q, nout, &dq, &host));
+    TRY(collide_cells_device(c, df, dq, nb, precision, cell0, cell1));
+    return finish(c, q, dq, nout, host);
+}
+
 int dgv_collide(dgv_ctx *ctx, const double *f, double *q, int64_t n, int precision)
 {
     if (!ctx) return DGV_EINVAL;

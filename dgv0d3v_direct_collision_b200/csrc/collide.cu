@@ -43,6 +43,7 @@ struct CollideArgs {
     int *err;               // raised by a bounded wait that gave up
     long long N;
     int Nc, Mv, Mw, nchunks, dcta, rowb;
+    int cell0, cell1;       // output cells evaluated: [cell0, cell1)
     int nst, sp;            // pipeline stages, pairs per stage
     int off_f, off_hdr, off_bar;  // shared-memory layout (bytes)
 };
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
     }
     __syncthreads();
     const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
-    const int d0 = slice * a.dcta, d1 = min(a.Nc, d0 + a.dcta);
+    const int d0 = a.cell0 + slice * a.dcta, d1 = min(a.cell1, d0 + a.dcta);
 
     if (threadIdx.x < 32) {  // producer: lane 0 of warp 0
         if (threadIdx.x == 0)
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
     // ---------------- consumers: one output cell D per thread ----------------
     const int tc = threadIdx.x - 32, lane = threadIdx.x & 31;
     const int D = d0 + tc;
-    const bool inD = tc < a.dcta && D < a.Nc;
+    const bool inD = tc < a.dcta && D < d1;
     const int Du = D / (a.Mv * a.Mw), Dv = (D / a.Mw) % a.Mv, Dw = D % a.Mw;
     const double *g = (MODE == MODE_BILINEAR) ? a.f2 + (size_t)vdf * a.N : nullptr;
     T acc[PV];
@@ -227,23 +228,25 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
     }
 }
 
-// q[v][D*P+p] = scale * (2 * sum_chunks partial[v][chunk][p][D]) / w[D*P+p]
+// q[v][D*P+p - cell0*P] = scale * (2 * sum_chunks partial[v][chunk][p][D]) / w[D*P+p]
+// for the output cells D in [cell0, cell1)
 __global__ void k_reduce_chunks(const double *partial, const double *w, double *q, int nchunks, int P, int Nc,
-                                long long N, int nvdf, double scale)
+                                int cell0, int cell1, int nvdf, double scale)
 {
+    const int ncell = cell1 - cell0;
+    const long long len = (long long)ncell * P;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long tot = (long long)nvdf * N;
-    if (idx >= tot) return;
-    int v = (int)(idx / N);
-    long long r = idx - (long long)v * N;
-    int p = (int)(r / Nc), D = (int)(r - (long long)p * Nc);  // D fastest: coalesced partial reads
+    if (idx >= (long long)nvdf * len) return;
+    int v = (int)(idx / len);
+    long long r = idx - (long long)v * len;
+    int p = (int)(r / ncell), D = cell0 + (int)(r - (long long)p * ncell);  // D fastest: coalesced partial reads
     const double *src = partial + ((size_t)v * nchunks * P + p) * Nc + D;
     double s = 0.0;
     for (int ch = 0; ch < nchunks; ch++) s += src[(size_t)ch * P * Nc];
     long long i = (long long)D * P + p;
     double val = 2.0 * s / w[i];
     if (scale != 1.0) val = val * scale;
-    q[(size_t)v * N + i] = val;
+    q[(size_t)v * len + (i - (long long)cell0 * P)] = val;
 }
 
 // -------------------------------------------------------------------------
@@ -273,7 +276,7 @@ struct LaunchShape {
 // Pipeline geometry: consumers = one warp per 32 output cells (<= 384), plus
 // the producer warp; the stage ring takes what shared memory the copy of f
 // leaves, up to 64 KiB, in 4-6 stages.
-static int shape_for(Ctx *c, int mode, LaunchShape &s)
+static int shape_for(Ctx *c, int mode, LaunchShape &s, int ncell)
 {
     const Grid &g = c->grid;
     const Layout &L = c->lay;
@@ -281,8 +284,8 @@ static int shape_for(Ctx *c, int mode, LaunchShape &s)
     DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     // at most 11 consumer warps + the producer: 12 warps = 3 per SM
     // sub-partition, which leaves 170 registers per thread (no spills)
-    s.slices = (g.Nc + 351) / 352;
-    s.dcta = ((g.Nc + s.slices - 1) / s.slices + 31) / 32 * 32;
+    s.slices = (ncell + 351) / 352;
+    s.dcta = ((ncell + s.slices - 1) / s.slices + 31) / 32 * 32;
     s.threads = 32 + s.dcta;
     const int rowb = mode == MODE_F32C ? L.RW32 * 4 : L.RD64 * 8;
     const size_t fbytes = (size_t)g.N * (mode == MODE_F32C ? sizeof(float) : sizeof(double));
@@ -301,7 +304,7 @@ static int shape_for(Ctx *c, int mode, LaunchShape &s)
 }
 
 static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_q, int nvdf, int precision,
-                       double scale, int nchunks)
+                       double scale, int nchunks, int cell0, int cell1)
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
@@ -309,7 +312,7 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     KernelFn fn = pick_kernel(g.P, mode);
     if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8 or 27 nodes per cell");
     LaunchShape sh;
-    int rc = shape_for(c, mode, sh);
+    int rc = shape_for(c, mode, sh, cell1 - cell0);
     if (rc) return rc;
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     nchunks = std::max(1, std::min<int>(nchunks, (int)std::max<long long>(1, L.nblocks)));
@@ -328,6 +331,7 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     a.rowb = mode == MODE_F32C ? L.RW32 * 4 : L.RD64 * 8;
     a.bounds = d_bounds; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw;
     a.nchunks = nchunks; a.dcta = sh.dcta; a.nst = sh.nst; a.sp = sh.sp;
+    a.cell0 = cell0; a.cell1 = cell1;
     a.off_f = sh.off_f; a.off_hdr = sh.off_hdr; a.off_bar = sh.off_bar;
     // VDF fastest: the CTAs resident at one time work on the same chunk of
     // rows for different VDFs, so each row is fetched from HBM once and then
@@ -336,9 +340,9 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     fn<<<dim3(nvdf, sh.slices, nchunks), sh.threads, sh.smem, c->stream>>>(a);
     kt.stop(1);
     DGV_CUDA(c, cudaGetLastError());
-    long long tot = (long long)nvdf * g.N;
-    k_reduce_chunks<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_partial, c->d_nwt, d_q, nchunks, g.P,
-                                                                             g.Nc, g.N, nvdf, scale);
+    const long long tot_out = (long long)nvdf * (cell1 - cell0) * g.P;
+    k_reduce_chunks<<<(unsigned)((tot_out + 255) / 256), 256, 0, c->stream>>>(c->d_partial, c->d_nwt, d_q, nchunks,
+                                                                                 g.P, g.Nc, cell0, cell1, nvdf, scale);
     DGV_CUDA(c, cudaGetLastError());
     count_launches(c, 2);
     return DGV_OK;
@@ -349,12 +353,14 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
 // CTAs balance it) whose last wave is at least 90% full (one CTA per SM: the
 // shared copy of f takes most of it).  Smaller batches: measured -- each
 // candidate is timed once and the fastest kept.
-static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *d_q, int nvdf, int precision)
+static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *d_q, int nvdf, int precision,
+                         int cell0, int cell1)
 {
     if (c->nchunks_opt > 0) return c->nchunks_opt;
     const Grid &g = c->grid;
     LaunchShape sh;
-    int rc0 = shape_for(c, d_f2 ? MODE_BILINEAR : (precision == DGV_PREC_F64 ? MODE_F64 : MODE_F32C), sh);
+    int rc0 = shape_for(c, d_f2 ? MODE_BILINEAR : (precision == DGV_PREC_F64 ? MODE_F64 : MODE_F32C), sh,
+                        cell1 - cell0);
     if (rc0) return 1;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
@@ -367,7 +373,8 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
         }
         return 64;
     }
-    long long key = ((long long)precision << 40) ^ ((long long)(d_f2 != nullptr) << 39) ^ nvdf;
+    long long key = ((long long)precision << 56) ^ ((long long)(d_f2 != nullptr) << 55) ^
+                    ((long long)cell0 << 38) ^ ((long long)cell1 << 21) ^ nvdf;
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) return it->second;
     int base = (int)std::max<long long>(1, (long long)nsm / units);
@@ -378,9 +385,9 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (int t = 0; t < 4; t++) {
-        if (run_collide(c, d_f, d_f2, d_q, nvdf, precision, 1.0, cand[t])) break;  // warm-up
+        if (run_collide(c, d_f, d_f2, d_q, nvdf, precision, 1.0, cand[t], cell0, cell1)) break;  // warm-up
         cudaEventRecord(e0, c->stream);
-        run_collide(c, d_f, d_f2, d_q, nvdf, precision, 1.0, cand[t]);
+        run_collide(c, d_f, d_f2, d_q, nvdf, precision, 1.0, cand[t], cell0, cell1);
         cudaEventRecord(e1, c->stream);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -400,21 +407,32 @@ int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precisi
     if (precision == DGV_PREC_TC) return collide_tc_device(c, d_f, d_q, nvdf, scale);
     if (precision != DGV_PREC_F64 && precision != DGV_PREC_F32C)
         return set_err(c, DGV_EINVAL, "collide: unknown precision");
-    int nch = choose_chunks(c, d_f, nullptr, d_q, nvdf, precision);
-    int rc = run_collide(c, d_f, nullptr, d_q, nvdf, precision, scale, nch);
+    int nch = choose_chunks(c, d_f, nullptr, d_q, nvdf, precision, 0, c->grid.Nc);
+    int rc = run_collide(c, d_f, nullptr, d_q, nvdf, precision, scale, nch, 0, c->grid.Nc);
     if (rc) return rc;
     if (c->project) return project_device(c, d_q, nvdf);
     return DGV_OK;
+}
+
+int collide_cells_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, int cell0, int cell1)
+{
+    if (!c->lay.blk) return set_err(c, DGV_ESTATE, "collide: no A-arrays loaded");
+    if (precision != DGV_PREC_F64 && precision != DGV_PREC_F32C)
+        return set_err(c, DGV_EUNSUP, "collide_cells: FP64 or FP32-compensated only");
+    if (cell0 < 0 || cell1 > c->grid.Nc || cell0 >= cell1)
+        return set_err(c, DGV_ERANGE, "collide_cells: cell range outside [0, Nc) or empty");
+    int nch = choose_chunks(c, d_f, nullptr, d_q, nvdf, precision, cell0, cell1);
+    return run_collide(c, d_f, nullptr, d_q, nvdf, precision, 1.0, nch, cell0, cell1);
 }
 
 int jvp_device(Ctx *c, const double *d_f, const double *d_df, double *d_q, int precision)
 {
     if (!c->lay.blk) return set_err(c, DGV_ESTATE, "jvp: no A-arrays loaded");
     (void)precision;
-    int nch = choose_chunks(c, d_f, d_df, d_q, 1, DGV_PREC_F64);
+    int nch = choose_chunks(c, d_f, d_df, d_q, 1, DGV_PREC_F64, 0, c->grid.Nc);
     // the bilinear kernel sums 2/w * A * (f g + g f) / 2 * 2: the reduce
     // kernel's factor 2 is the reference's "2*fc/w" (collision_mod.f90:326)
-    return run_collide(c, d_f, d_df, d_q, 1, DGV_PREC_F64, 1.0, nch);
+    return run_collide(c, d_f, d_df, d_q, 1, DGV_PREC_F64, 1.0, nch, 0, c->grid.Nc);
 }
 
 }  // namespace dgv

@@ -160,6 +160,7 @@ int get_chunks(Ctx *c, int nchunks, int **d_bounds);
 int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision,
                    double scale);
 int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale);
+int collide_cells_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, int cell0, int cell1);
 int jvp_device(Ctx *c, const double *d_f, const double *d_df, double *d_q, int precision);
 int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int precision);
 int moments_device(Ctx *c, const double *d_f, int nvdf, double *h_out);

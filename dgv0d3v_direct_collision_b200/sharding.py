@@ -43,3 +43,37 @@ def gather_node_slices(q_local, Nc: int, P: int, group=None):
     out = [torch.empty_like(buf) for _ in range(world)]
     dist.all_gather(out, buf, group=group)
     return torch.cat([o[: b - a] for o, (a, b) in zip(out, sizes)])
+
+
+def sharded_collide(solver, f, group=None, precision: str = "f64"):
+    """Q(f,f) of one VDF split over the ranks of `group` by output cells:
+    every rank holds the full f and A, evaluates its balanced share of cells
+    (dgv_collide_cells) and one all-gather assembles Q on every rank."""
+    import torch
+    import torch.distributed as dist
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    c0, c1 = balanced_range(solver.Nc, world, rank)
+    if f.is_cuda:  # the library runs on its own stream; f may still be in flight on torch's
+        torch.cuda.current_stream(f.device).synchronize()
+    q_local = solver.collide_cells(f.contiguous(), c0, c1, precision=precision)
+    return gather_node_slices(q_local, solver.Nc, solver.P, group)
+
+
+def sharded_rk_step(solver, f, dt: float, order: int = 2, group=None, precision: str = "f64"):
+    """One RK step (the reference's schemes, explicit stage form) of a single
+    VDF sharded by output cells: one all-gather per stage, f replicated."""
+    from .autograd import RK_TABLEAUX
+    A, B = RK_TABLEAUX[order]
+    h = solver.kappa * dt
+    ks = []
+    for i in range(len(A)):
+        s = f
+        for j, a in enumerate(A[i]):
+            if a != 0.0:
+                s = s + a * ks[j]
+        ks.append(h * sharded_collide(solver, s, group, precision))
+    out = f
+    for b, k in zip(B, ks):
+        if b != 0.0:
+            out = out + b * k
+    return out

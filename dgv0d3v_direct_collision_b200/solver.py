@@ -187,6 +187,24 @@ class DGVSolver:
 
     collide = EvalCollisionPeriodicAPlus_DGV
 
+    def collide_cells(self, f, cell0: int, cell1: int, out=None, precision=None):
+        """Q on output cells [cell0, cell1) only (one rank's share of a sharded
+        evaluation): returns (..., (cell1-cell0)*P) in node order."""
+        _check_f64(f)
+        nb = int(np.prod(f.shape)) // self.N
+        if nb * self.N != int(np.prod(f.shape)):
+            raise ValueError(f"f must hold a multiple of {self.N} values")
+        shape = tuple(f.shape[:-1]) + ((cell1 - cell0) * self.P,)
+        if out is None:
+            if isinstance(f, np.ndarray):
+                out = np.zeros(shape)
+            else:
+                import torch
+                out = torch.zeros(shape, dtype=torch.float64, device=f.device)
+        self._check(self._lib.dgv_collide_cells(self._h, nb, _ptr(f), _ptr(out), int(cell0), int(cell1),
+                                                self._prec(precision)))
+        return out
+
     def EvalCollisionPeriodicMixedTermsA_DGV(self, f, fm, fc=None):
         """2/w sum A (fm(xi) f(xi1) + f(xi) fm(xi1)): the JVP of Q at fm along f."""
         _check_f64(f); _check_f64(fm)

@@ -127,6 +127,14 @@ int dgv_collide(dgv_ctx *ctx, const double *f, double *q, int64_t n, int precisi
 int dgv_collide_batched(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int precision);
 /* fcol = kappa*dt*Q(f,f) (SpatialOperSH_DGV, spat_oper_mod.f90:28-68, run_mode 0) */
 int dgv_spatial_oper(dgv_ctx *ctx, const double *f, double *fcol, double dt, int precision);
+/* Q on the output cells [cell0, cell1) only: q[nb][(cell1-cell0)*P], node
+ * order within the range.  The MPI split of output nodes over ranks
+ * (miscmpiset.f90:195-200, 1017-1098; each rank's share of the loop of
+ * collision_mod.f90:186-227): one rank of a sharded single-VDF run evaluates
+ * its cells and the slices are gathered.  FP64 or FP32-compensated; no
+ * conservation projection (it needs the whole Q). */
+int dgv_collide_cells(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int32_t cell0, int32_t cell1,
+                      int precision);
 /* No counterpart in the reference.  q = Q(f,f) in FP64, as dgv_collide_batched,
  * for callers that cannot allocate device memory once they are running -- a
  * driver that gives all free memory to its own pool allocator at start-up, or
