@@ -25,6 +25,7 @@ BUILD = os.path.join(HERE, "_build")
 SOURCES = [
     ("grid.cpp", []),
     ("layout.cpp", []),
+    ("afile.cpp", []),
     ("api.cu", []),
     ("collide.cu", []),
     ("collide_tc.cu", []),

@@ -158,6 +158,17 @@ class DGVSolver:
     def generate_synthetic_A(self, seed: int = 1, Trad: float = float("inf"), support: int = 1):
         self._check(self._lib.dgv_generate_A_synthetic(self._h, seed, Trad, support))
 
+    def read_A_files(self, paths):
+        """Load an operator file (or the chunk files of one operator) in the
+        reference's format (ReadAarraysDGV / ReadAarraysChnksDGV)."""
+        from .afile import _paths
+        arr, n = _paths(paths)
+        self._check(self._lib.dgv_read_A_files(self._h, arr, n))
+
+    def write_A_file(self, path: str, max_subrecord: int = 0):
+        """Write the loaded A-arrays as one operator file (WriteAarraysDGV)."""
+        self._check(self._lib.dgv_write_A_file(self._h, path.encode(), int(max_subrecord)))
+
     def A_info(self):
         nr = C.c_int64(); npairs = C.c_int64(); nb = C.c_int64(); rs = C.c_double()
         self._check(self._lib.dgv_A_info(self._h, C.byref(nr), C.byref(npairs), C.byref(nb),

@@ -119,6 +119,32 @@ int dgv_A_info(const dgv_ctx *ctx, int64_t *nrecords, int64_t *npairs, int64_t *
 int dgv_export_A(const dgv_ctx *ctx, int64_t *nnz_out, int32_t *capphi, double *A,
                  int32_t *A_xi, int32_t *A_xi1);
 
+/* -- A-array files (the reference's on-disk operator) --------------------- */
+/* Reads the A-arrays of an operator file (WriteAarraysDGV's format,
+ * readwrite.f90:1459-1484: a Fortran unformatted sequential file of the
+ * records (mm, nn) and (A_capphi, A, A_xi, A_xi1, A_phi), gfortran record
+ * framing, subrecords for records over 2^31-9 bytes), or of a chunked
+ * operator split over nfiles files (ReadAarraysChnksDGV,
+ * readwrite.f90:1130-1243: A_capphi summed, records concatenated in file
+ * order), and loads them into the context as dgv_load_A does. */
+int dgv_read_A_files(dgv_ctx *ctx, const char *const *paths, int32_t nfiles);
+/* Writes the loaded A-arrays as one operator file in that format
+ * (WriteAarraysDGV, readwrite.f90:1459-1484); max_subrecord = 0 for
+ * gfortran's limit, a smaller positive value splits records sooner. */
+int dgv_write_A_file(dgv_ctx *ctx, const char *path, int64_t max_subrecord);
+/* The same reader without a context or a GPU (ReadAarraysChnksDGV,
+ * readwrite.f90:1130-1243): fills caller arrays, indices 1-based as stored;
+ * NULL arrays query nnz_out only.  Errors: dgv_file_error(). */
+int dgv_read_A_arrays(const char *const *paths, int32_t nfiles, int32_t N, int64_t *nnz_out,
+                      int32_t *capphi, double *A, int32_t *A_xi, int32_t *A_xi1);
+/* The same writer from caller arrays (WriteAarraysDGV, readwrite.f90:1459-1484),
+ * indices 1-based; A_phi is derived from capphi. */
+int dgv_write_A_arrays(const char *path, int32_t N, int64_t nnz, const int32_t *capphi, const double *A,
+                       const int32_t *A_xi, const int32_t *A_xi1, int64_t max_subrecord);
+/* message of the last failing dgv_read_A_arrays / dgv_write_A_arrays on this
+ * thread (the file routines of readwrite.f90:1066-1484 stop on errors) */
+const char *dgv_file_error(void);
+
 /* -- collision operator --------------------------------------------------- */
 /* q = Q(f,f) (EvalCollisionPeriodicAPlus_DGV, collision_mod.f90:143-229);
  * n must equal N. */
