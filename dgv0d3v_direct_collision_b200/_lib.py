@@ -25,7 +25,7 @@ EXPORTS = [
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper",
     "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
     "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
-    "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
+    "dgv_compute_A", "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
 ]
 
 
@@ -73,6 +73,7 @@ def load() -> C.CDLL:
         "dgv_collide": [vp, vp, vp, i64, C.c_int],
         "dgv_collide_batched": [vp, i32, vp, vp, C.c_int],
         "dgv_collide_cells": [vp, i32, vp, vp, i32, i32, C.c_int],
+        "dgv_compute_A": [vp, dbl, dbl, dbl, dbl, C.c_int],
         "dgv_read_A_files": [vp, C.POINTER(C.c_char_p), i32],
         "dgv_write_A_file": [vp, C.c_char_p, i64],
         "dgv_read_A_arrays": [C.POINTER(C.c_char_p), i32, i32, C.POINTER(i64), vp, vp, vp, vp],

@@ -32,6 +32,7 @@ SOURCES = [
     ("adjoint.cu", []),
     ("noalloc.cu", []),
     ("synth.cu", ["-fmad=false"]),
+    ("seta.cu", ["-fmad=false"]),
     ("stepping.cu", ["-fmad=false"]),
 ]
 

@@ -383,6 +383,16 @@ int dgv_generate_A_synthetic(dgv_ctx *ctx, uint64_t seed, double Trad, int suppo
     return layout_synthetic(c, seed, Trad, support_mode);
 }
 
+int dgv_compute_A(dgv_ctx *ctx, double Trad, double ErrChi, double ErrEps, double min_sens, int basis_mode)
+{
+    CTX_CHECK(ctx);
+    Ctx *c = &ctx->c;
+    DGV_CUDA(c, cudaSetDevice(c->device));
+    release_graphs(c);
+    TRY(layout_seta(c, Trad, ErrChi, ErrEps, min_sens, basis_mode));
+    return DGV_OK;
+}
+
 int dgv_A_info(const dgv_ctx *ctx, int64_t *nrecords, int64_t *npairs, int64_t *nblocks, double *record_shifts)
 {
     if (!ctx) return DGV_EINVAL;

@@ -152,6 +152,7 @@ int check_errflag(Ctx *c);
 int layout_from_reference(Ctx *c, long long nnz, const int32_t *capphi, const double *A,
                           const int32_t *xi, const int32_t *xi1, int one_based);
 int layout_synthetic(Ctx *c, unsigned long long seed, double Trad, int support_mode);
+int layout_seta(Ctx *c, double Trad, double ErrChi, double ErrEps, double min_sens, int basis_mode);
 int layout_export(Ctx *c, long long *nnz_out, int32_t *capphi, double *A, int32_t *xi,
                   int32_t *xi1);
 int get_chunks(Ctx *c, int nchunks, int **d_bounds);

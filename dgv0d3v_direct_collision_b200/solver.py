@@ -158,6 +158,15 @@ class DGVSolver:
     def generate_synthetic_A(self, seed: int = 1, Trad: float = float("inf"), support: int = 1):
         self._check(self._lib.dgv_generate_A_synthetic(self._h, seed, Trad, support))
 
+    def SetA_DGV(self, Trad: float = float("inf"), ErrChi: float = 1e-4, ErrEps: float = 1e-4,
+                 min_sens: float = 0.0, basis_mode: int = 0):
+        """Compute the A-arrays of every canonical basis function on the GPU
+        (the reference's SetA_DGV precompute) and load them."""
+        self._check(self._lib.dgv_compute_A(self._h, float(Trad), float(ErrChi), float(ErrEps),
+                                            float(min_sens), int(basis_mode)))
+
+    compute_A = SetA_DGV
+
     def read_A_files(self, paths):
         """Load an operator file (or the chunk files of one operator) in the
         reference's format (ReadAarraysDGV / ReadAarraysChnksDGV)."""

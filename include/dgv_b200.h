@@ -109,6 +109,17 @@ int dgv_load_A(dgv_ctx *ctx, int64_t nnz, const int32_t *capphi, const double *A
  * (seed, p, xi, xi1) in [-1,1).  No reference counterpart: a seeded stand-in
  * for A-arrays that take hours to precompute. */
 int dgv_generate_A_synthetic(dgv_ctx *ctx, uint64_t seed, double Trad, int support_mode);
+/* Computes the A-arrays on the device: SetA_DGV (dgvtools_mod.f90:377-681,
+ * with A_IntEpsilon :988-1122 and EvalPhiPostCollIntegrand :938-975) for every
+ * basis function of the canonical cell -- nested adaptive Simpson integrals
+ * over the collision sphere of every pair xi < xi1 passing the prefilter
+ * (cutoff Trad), tolerances ErrChi (chi) and ErrEps (eps), records with
+ * |A| > min_sens kept.  basis_mode 0 is the Lagrange basis with the
+ * commented lines of :254-287 restored; 1..5 put the collision invariants
+ * 1, u, v, w, |v|^2 in place of the basis function (the known-answer test
+ * of :267-274: every record ~ 0).  Replaces the precompute whose output
+ * ReadAarraysDGV reads. */
+int dgv_compute_A(dgv_ctx *ctx, double Trad, double ErrChi, double ErrEps, double min_sens, int basis_mode);
 /* counts of the loaded A-arrays: records, distinct (xi,xi1) pairs, cell-pair
  * blocks, and record-shift visits per Q evaluation */
 int dgv_A_info(const dgv_ctx *ctx, int64_t *nrecords, int64_t *npairs, int64_t *nblocks,
