@@ -22,7 +22,8 @@ STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4
 EXPORTS = [
     "dgv_ctx_create", "dgv_ctx_destroy", "dgv_last_error", "dgv_set_stream", "dgv_set_async",
     "dgv_set_option", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
-    "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper",
+    "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper", "dgv_set_regime",
+    "dgv_regime_info",
     "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
     "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
     "dgv_compute_A", "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
@@ -78,6 +79,8 @@ def load() -> C.CDLL:
         "dgv_write_A_file": [vp, C.c_char_p, i64],
         "dgv_read_A_arrays": [C.POINTER(C.c_char_p), i32, i32, C.POINTER(i64), vp, vp, vp, vp],
         "dgv_write_A_arrays": [C.c_char_p, i32, i64, vp, vp, vp, vp, i64],
+        "dgv_set_regime": [vp, dbl, dbl],
+        "dgv_regime_info": [vp, C.POINTER(i32), C.POINTER(dbl)],
         "dgv_spatial_oper": [vp, vp, vp, dbl, C.c_int],
         "dgv_step_rk": [vp, vp, vp, dbl, C.c_int, C.c_int],
         "dgv_prepare_ab": [vp, vp, dbl, C.c_int, C.c_int],

@@ -153,7 +153,7 @@ static void destroy_ctx(Ctx *c)
     free_ktimers(c);
     free_layout(c->lay);
     double *bufs[] = {c->d_nu, c->d_nv, c->d_nw, c->d_nwt, c->d_partial, c->d_in, c->d_out, c->d_red, c->d_fm,
-                      c->d_tcF, c->d_tcQ, c->d_glm};
+                      c->d_tcF, c->d_tcQ, c->d_glm, c->d_fmn, c->d_dfr, c->d_rgt};
     for (double *p : bufs)
         if (p) cudaFree(p);
     for (double *p : c->d_tmp)
@@ -340,6 +340,27 @@ int dgv_kernel_stats(dgv_ctx *ctx, double *ms, int64_t *launches, int64_t *all_l
     return DGV_OK;
 }
 
+int dgv_set_regime(dgv_ctx *ctx, double decomp_lev, double linear_lev)
+{
+    CTX_CHECK(ctx);
+    Ctx *c = &ctx->c;
+    if (decomp_lev < 0.0 || linear_lev < 0.0) return set_err(c, DGV_EINVAL, "set_regime: levels must be >= 0");
+    release_graphs(c);
+    c->decomp_lev = decomp_lev;
+    c->linear_lev = linear_lev;
+    c->run_mode = 0;
+    c->last_L1 = -1.0;
+    return DGV_OK;
+}
+
+int dgv_regime_info(const dgv_ctx *ctx, int32_t *run_mode, double *last_L1)
+{
+    if (!ctx) return DGV_EINVAL;
+    if (run_mode) *run_mode = ctx->c.run_mode;
+    if (last_L1) *last_L1 = ctx->c.last_L1;
+    return DGV_OK;
+}
+
 int dgv_grid_info(const dgv_ctx *ctx, int64_t *N, int32_t *P, int32_t *Nc, int32_t *ccell)
 {
     if (!ctx) return DGV_EINVAL;
@@ -467,7 +488,7 @@ int dgv_spatial_oper(dgv_ctx *ctx, const double *f, double *fcol, double dt, int
     bool host = false;
     TRY(stage_in(c, f, n, 0, &df));
     TRY(out_ptr(c, fcol, n, &dq, &host));
-    TRY(collide_device(c, df, dq, 1, precision, c->grid.d.kappa * dt));
+    TRY(spatial_device(c, df, dq, dt, precision));
     return finish(c, fcol, dq, n, host);
 }
 

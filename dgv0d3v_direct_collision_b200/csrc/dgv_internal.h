@@ -108,6 +108,12 @@ struct Ctx {
     int ab_order = 0;
     // linearisation point
     double *d_fm = nullptr;
+    // run modes of SpatialOperSH_DGV (CheckSolutionMode_DGV): off while
+    // decomp_lev == 0; the local Maxwellian, Df = f - fm and a scratch array
+    double decomp_lev = 0.0, linear_lev = 0.0, last_L1 = -1.0;
+    int run_mode = 0;
+    double *d_fmn = nullptr, *d_dfr = nullptr, *d_rgt = nullptr;
+    size_t fmn_bytes = 0, dfr_bytes = 0, rgt_bytes = 0;
     // error flag raised by a bounded device wait that gave up: pinned host
     // memory mapped into the device (h_err and d_err alias the same int)
     int *h_err = nullptr, *d_err = nullptr;
@@ -168,6 +174,7 @@ int moments_device(Ctx *c, const double *d_f, int nvdf, double *h_out);
 int project_device(Ctx *c, double *d_q, int nvdf);
 int maxwellian_device(Ctx *c, double T, double u0, double v0, double w0, double n, double *d_f);
 int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, int precision);
+int spatial_device(Ctx *c, const double *d_f, double *d_out, double dt, int precision);
 int ab_prepare_device(Ctx *c, double *d_f, double dt, int order, int precision);
 int ab_step_device(Ctx *c, double *d_f, double dt, int precision);
 

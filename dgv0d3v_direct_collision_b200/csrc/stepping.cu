@@ -248,10 +248,116 @@ static int ensure_tmp(Ctx *c)
     } while (0)
 
 // SpatialOperSH_DGV (spat_oper_mod.f90:28-68), run_mode 0: Q scaled by kappa*dt
+// sum_i |a_i - b_i| w_i: NPART fixed CTAs, fixed-order trees
+__global__ void k_wl1(const double *a, const double *b, const double *w, long long N, double *part)
+{
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * RED_THREADS + threadIdx.x; i < N; i += (long long)NPART * RED_THREADS)
+        s = s + fabs(a[i] - b[i]) * w[i];
+    __shared__ double sh[RED_THREADS];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = RED_THREADS / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// y = (a - b), or y = (a + b) * s, or y = a * s
+__global__ void k_regime_combine(double *y, const double *a, const double *b, double s, int op, long long N)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (op == 0) y[i] = a[i] - b[i];
+    else if (op == 1) y[i] = (a[i] + b[i]) * s;
+    else y[i] = a[i] * s;
+}
+
+static int wl1(Ctx *c, const double *a, const double *b, double *out)
+{
+    TRY(ensure_red(c, 1));
+    k_wl1<<<NPART, RED_THREADS, 0, c->stream>>>(a, b, c->d_nwt, c->grid.N, c->d_red);
+    DGV_CUDA(c, cudaGetLastError());
+    double part[NPART];
+    DGV_CUDA(c, cudaMemcpyAsync(part, c->d_red, sizeof(part), cudaMemcpyDeviceToHost, c->stream));
+    DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    double s = 0.0;
+    for (int b2 = 0; b2 < NPART; b2++) s += part[b2];
+    *out = s;
+    return DGV_OK;
+}
+
+static int combine(Ctx *c, double *y, const double *a, const double *b, double s, int op)
+{
+    const long long N = c->grid.N;
+    k_regime_combine<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(y, a, b, s, op, N);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 1);
+    return DGV_OK;
+}
+
+// SpatialOperSH_DGV (spat_oper_mod.f90:28-68) with CheckSolutionMode_DGV
+// (:195-272): the local Maxwellian fMN of f and the relative L1 distance
+// sum |f - fMN| w / n decide the run mode -- 0 far from equilibrium: Q(f);
+// 1 (distance < decomp_lev): L(Df) + Q(Df); 2 (distance < linear_lev): L(Df)
+// only, Df = f - fm, L the linearised operator at fm (the mixed terms at fm,
+// = 2 MATMUL(Df, fmA) of EvalCollisionLinear).  fm is replaced by fMN when a
+// mode is entered from 0 or when it has drifted more than linear_lev/2 from
+// fMN.  All times kappa*dt.  With decomp_lev = 0 the mode stays 0 (plain Q).
+int spatial_device(Ctx *c, const double *x, double *out, double dt, int precision)
+{
+    const double coef = c->grid.d.kappa * dt;
+    if (!(c->decomp_lev > 0.0)) return collide_device(c, x, out, 1, precision, coef);
+    const size_t nb = sizeof(double) * (size_t)c->grid.N;
+    TRY(ensure_buffer(c, &c->d_fmn, &c->fmn_bytes, nb));
+    TRY(ensure_buffer(c, &c->d_dfr, &c->dfr_bytes, nb));
+    TRY(ensure_buffer(c, &c->d_rgt, &c->rgt_bytes, nb));
+    if (!c->d_fm) DGV_CUDA(c, cudaMalloc(&c->d_fm, nb));
+    double m[5];
+    TRY(moments_device(c, x, 1, m));
+    TRY(maxwellian_device(c, m[4], m[1], m[2], m[3], m[0], c->d_fmn));
+    double L1 = 0.0;
+    TRY(wl1(c, x, c->d_fmn, &L1));
+    L1 = L1 / m[0];
+    c->last_L1 = L1;
+    if (L1 < c->decomp_lev) {
+        bool refresh = false;
+        if (c->run_mode == 0) {
+            refresh = true;
+            c->run_mode = L1 < c->linear_lev ? 2 : 1;
+        } else {
+            double L1fm = 0.0;
+            TRY(wl1(c, c->d_fm, c->d_fmn, &L1fm));
+            L1fm = L1fm / m[0];
+            if (L1fm > c->linear_lev / 2.0) refresh = true;
+            if (c->run_mode == 1 && L1 < c->linear_lev) c->run_mode = 2;
+            else if (c->run_mode == 2 && L1 > c->linear_lev) c->run_mode = 1;
+        }
+        if (refresh) DGV_CUDA(c, cudaMemcpyAsync(c->d_fm, c->d_fmn, nb, cudaMemcpyDeviceToDevice, c->stream));
+        TRY(combine(c, c->d_dfr, x, c->d_fm, 0.0, 0));
+    } else {
+        c->run_mode = 0;
+    }
+    if (c->run_mode == 0) return collide_device(c, x, out, 1, precision, coef);
+    const bool proj = c->project;
+    c->project = false;
+    int rc = jvp_device(c, c->d_fm, c->d_dfr, c->run_mode == 1 ? c->d_rgt : out, DGV_PREC_F64);
+    if (!rc && c->run_mode == 1) {
+        rc = collide_device(c, c->d_dfr, out, 1, precision, 1.0);
+        if (!rc) rc = combine(c, out, out, c->d_rgt, coef, 1);  // (Q(Df) + L(Df)) * kappa dt
+    } else if (!rc) {
+        rc = combine(c, out, out, nullptr, coef, 2);
+    }
+    c->project = proj;
+    if (rc) return rc;
+    if (proj) return project_device(c, out, 1);
+    return DGV_OK;
+}
+
 static int spatial(Ctx *c, const double *x, double *out, double dt, int precision)
 {
-    double coef = c->grid.d.kappa * dt;
-    return collide_device(c, x, out, 1, precision, coef);
+    return spatial_device(c, x, out, dt, precision);
 }
 
 // one RK step of the given order; d_r1 receives frhs1 (already divided by dt)
@@ -343,6 +449,9 @@ int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, i
     if (order < 1 || order > 5) return set_err(c, DGV_EINVAL, "step_rk: order must be 1..5");
     TRY(ensure_tmp(c));
     double *r1 = d_frhs1 ? d_frhs1 : c->d_tmp[4];
+    // with run modes the mode check synchronises on the host at every stage:
+    // no graph capture
+    if (c->decomp_lev > 0.0) return rk_body(c, d_f, r1, dt, order, precision);
     RkGraphKey key;
     std::memset(&key, 0, sizeof(key));
     key.f = d_f; key.r1 = r1; key.dt = dt; key.order = order; key.precision = precision; key.project = c->project;

@@ -124,6 +124,16 @@ class DGVSolver:
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_PROJECT, int(on)))
         self.projection = bool(on)
 
+    def set_regime(self, decomp_lev: float, linear_lev: float):
+        """Run modes of SpatialOperSH_DGV (CheckSolutionMode_DGV); decomp_lev = 0 switches them off."""
+        self._check(self._lib.dgv_set_regime(self._h, float(decomp_lev), float(linear_lev)))
+
+    def regime_info(self):
+        """(run_mode, last relative L1 distance of f to its local Maxwellian)"""
+        m, l1 = C.c_int32(), C.c_double()
+        self._check(self._lib.dgv_regime_info(self._h, C.byref(m), C.byref(l1)))
+        return m.value, l1.value
+
     def set_nchunks(self, n: int):
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_NCHUNKS, int(n)))
 

@@ -162,8 +162,23 @@ const char *dgv_file_error(void);
 int dgv_collide(dgv_ctx *ctx, const double *f, double *q, int64_t n, int precision);
 /* nb VDFs stored contiguously, f[nb][N] -> q[nb][N] */
 int dgv_collide_batched(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int precision);
-/* fcol = kappa*dt*Q(f,f) (SpatialOperSH_DGV, spat_oper_mod.f90:28-68, run_mode 0) */
+/* fcol = kappa*dt*Q(f,f) (SpatialOperSH_DGV, spat_oper_mod.f90:28-68); with
+ * run modes switched on (dgv_set_regime) the mode of CheckSolutionMode_DGV
+ * decides: Q(f), L(Df) + Q(Df) or L(Df), Df = f - fm */
 int dgv_spatial_oper(dgv_ctx *ctx, const double *f, double *fcol, double dt, int precision);
+/* Switches on the run modes of SpatialOperSH_DGV for dgv_spatial_oper and the
+ * RK / AB steps (CheckSolutionMode_DGV, spat_oper_mod.f90:195-272, levels
+ * decomp_lev and linear_lev of commvar): relative L1 distance of f to its
+ * local Maxwellian below decomp_lev -> decomposition (mode 1), below
+ * linear_lev -> linearised (mode 2), else the full operator (mode 0).
+ * decomp_lev = 0 switches them off.  Resets the mode to 0; the mode's
+ * linearisation point fm is also the one dgv_apply_linear uses.  RK steps
+ * are not captured into graphs while modes are on. */
+int dgv_set_regime(dgv_ctx *ctx, double decomp_lev, double linear_lev);
+/* current run_mode and the last relative L1 distance (-1 before the first
+ * check), as CheckSolutionMode_DGV (spat_oper_mod.f90:195-272) and
+ * KeepTrackL1_err_DGV record them */
+int dgv_regime_info(const dgv_ctx *ctx, int32_t *run_mode, double *last_L1);
 /* Q on the output cells [cell0, cell1) only: q[nb][(cell1-cell0)*P], node
  * order within the range.  The MPI split of output nodes over ranks
  * (miscmpiset.f90:195-200, 1017-1098; each rank's share of the loop of

@@ -505,9 +505,115 @@ void dgvo_spatial_oper(const dgvo_ctx *c, const double *f, double *fcol, double 
     for (int64_t i = 0; i < c->N; i++) fcol[i] = fcol[i] * coef;
 }
 
+/* Regime state of SpatialOperSH_DGV (run_mode, fm; spat_oper_mod.f90:28-68) */
+struct dgvo_regime {
+    int run_mode;
+    double decomp_lev, linear_lev, last_L1;
+    double *fm;
+};
+
+dgvo_regime *dgvo_regime_create(const dgvo_ctx *c, double decomp_lev, double linear_lev)
+{
+    dgvo_regime *r = calloc(1, sizeof(dgvo_regime));
+    r->decomp_lev = decomp_lev;
+    r->linear_lev = linear_lev;
+    r->last_L1 = -1.0;
+    r->fm = calloc((size_t)c->N, sizeof(double));
+    return r;
+}
+
+void dgvo_regime_free(dgvo_regime *r)
+{
+    if (!r) return;
+    free(r->fm);
+    free(r);
+}
+
+int dgvo_regime_mode(const dgvo_regime *r, double *last_L1)
+{
+    if (last_L1) *last_L1 = r->last_L1;
+    return r->run_mode;
+}
+
+/* CheckSolutionMode_DGV (spat_oper_mod.f90:195-272): the local Maxwellian of
+ * f, the relative L1 distance to it, the run_mode switch and the refresh of
+ * fm (PrepareFMA_DGV: here fm itself -- the linear part is evaluated as the
+ * mixed terms at fm, equal to 2*MATMUL(Df, fmA)); Df = f - fm */
+static void check_mode(const dgvo_ctx *c, dgvo_regime *r, const double *f, double *Df)
+{
+    int64_t N = c->N, i;
+    double m[5];
+    dgvo_moments(c, f, m);
+    double *fmn = malloc(sizeof(double) * N);
+    dgvo_maxwellian(c, m[4], m[1], m[2], m[3], m[0], fmn);
+    double L1 = 0.0;
+    for (i = 0; i < N; i++) L1 = L1 + fabs(f[i] - fmn[i]) * c->nwt[i];
+    L1 = L1 / m[0];
+    r->last_L1 = L1;
+    if (L1 < r->decomp_lev) {
+        double L1fm;
+        switch (r->run_mode) {
+        case 0:
+            memcpy(r->fm, fmn, sizeof(double) * N);
+            r->run_mode = L1 < r->linear_lev ? 2 : 1;
+            break;
+        case 1:
+        case 2:
+            L1fm = 0.0;
+            for (i = 0; i < N; i++) L1fm = L1fm + fabs(r->fm[i] - fmn[i]) * c->nwt[i];
+            L1fm = L1fm / m[0];
+            if (L1fm > r->linear_lev / 2.0) memcpy(r->fm, fmn, sizeof(double) * N);
+            if (r->run_mode == 1 && L1 < r->linear_lev) r->run_mode = 2;
+            else if (r->run_mode == 2 && L1 > r->linear_lev) r->run_mode = 1;
+            break;
+        }
+        for (i = 0; i < N; i++) Df[i] = f[i] - r->fm[i];
+    } else {
+        r->run_mode = 0;
+    }
+    free(fmn);
+}
+
+/* SpatialOperSH_DGV (spat_oper_mod.f90:28-68) with its run modes: 0 Q(f),
+ * 1 L(Df) + Q(Df), 2 L(Df); times kappa*dt.  r == NULL: mode 0 always. */
+void dgvo_spatial_oper_regime(const dgvo_ctx *c, dgvo_regime *r, const double *f, double *fcol, double dt,
+                              double kappa, int nthreads)
+{
+    if (!r) {
+        dgvo_spatial_oper(c, f, fcol, dt, kappa, nthreads);
+        return;
+    }
+    int64_t N = c->N, i;
+    double *Df = malloc(sizeof(double) * N), *scr = malloc(sizeof(double) * N);
+    check_mode(c, r, f, Df);
+    switch (r->run_mode) {
+    case 0:
+        dgvo_collide_aplus(c, f, fcol, NULL, 0, nthreads);
+        break;
+    case 1:
+        dgvo_mixed_terms(c, Df, r->fm, scr, nthreads);
+        dgvo_collide_aplus(c, Df, fcol, NULL, 0, nthreads);
+        for (i = 0; i < N; i++) fcol[i] = fcol[i] + scr[i];
+        break;
+    default:
+        dgvo_mixed_terms(c, Df, r->fm, fcol, nthreads);
+        break;
+    }
+    double coef = kappa * dt;
+    for (i = 0; i < N; i++) fcol[i] = fcol[i] * coef;
+    free(Df);
+    free(scr);
+}
+
 /* TimeIntegratorORK_SH_DGV (time_integr_mod.f90:26-152) */
 int dgvo_rk_step(const dgvo_ctx *c, int order, double *f, double *frhs1, double dt,
                  double kappa, int nthreads)
+{
+    return dgvo_rk_step_regime(c, NULL, order, f, frhs1, dt, kappa, nthreads);
+}
+
+int dgvo_rk_step_regime(const dgvo_ctx *c, dgvo_regime *reg, int order, double *f, double *frhs1, double dt,
+                        double kappa, int nthreads)
 {
     int64_t N = c->N;
     if (order < 1 || order > 5) return 1;
@@ -516,47 +622,47 @@ int dgvo_rk_step(const dgvo_ctx *c, int order, double *f, double *frhs1, double 
     int64_t i;
     switch (order) {
     case 1:
-        dgvo_spatial_oper(c, f, frhs1, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, f, frhs1, dt, kappa, nthreads);
         for (i = 0; i < N; i++) f[i] = f[i] + frhs1[i];
         break;
     case 2: /* :55-59 */
-        dgvo_spatial_oper(c, f, frhs1, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, f, frhs1, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] * 2 / 3.0;
-        dgvo_spatial_oper(c, t0, ft2, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft2, dt, kappa, nthreads);
         for (i = 0; i < N; i++) f[i] = f[i] + frhs1[i] / 4.0 + ft2[i] * 3.0 / 4;
         break;
     case 3: /* :76-82 */
-        dgvo_spatial_oper(c, f, frhs1, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, f, frhs1, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] / 2.0;
-        dgvo_spatial_oper(c, t0, ft2, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft2, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + ft2[i] * 3.0 / 4;
-        dgvo_spatial_oper(c, t0, ft3, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft3, dt, kappa, nthreads);
         for (i = 0; i < N; i++) f[i] = f[i] + frhs1[i] * 2 / 9.0 + ft2[i] * 3.0 / 9.0 + ft3[i] * 4 / 9.0;
         break;
     case 4: /* :95-104 */
-        dgvo_spatial_oper(c, f, frhs1, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, f, frhs1, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] / 2.0;
-        dgvo_spatial_oper(c, t0, ft2, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft2, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] / 4.0 + ft2[i] / 4.0;
-        dgvo_spatial_oper(c, t0, ft3, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft3, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] - ft2[i] + ft3[i] * 2;
-        dgvo_spatial_oper(c, t0, ft2, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft2, dt, kappa, nthreads);
         for (i = 0; i < N; i++) f[i] = f[i] + frhs1[i] / 6.0 + ft3[i] * 2 / 3.0 + ft2[i] / 6.0;
         break;
     case 5: /* :122-146 */
-        dgvo_spatial_oper(c, f, frhs1, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, f, frhs1, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] / 2.0;
-        dgvo_spatial_oper(c, t0, ft2, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft2, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] / 4.0 + ft2[i] / 4.0;
-        dgvo_spatial_oper(c, t0, ft3, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft3, dt, kappa, nthreads);
         for (i = 0; i < N; i++) t0[i] = f[i] - ft2[i] + ft3[i] * 2.0;
-        dgvo_spatial_oper(c, t0, ft4, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft4, dt, kappa, nthreads);
         for (i = 0; i < N; i++) ft3[i] = -ft2[i] / 5.0 + ft3[i] * 546 / 625.0;
         for (i = 0; i < N; i++) t0[i] = f[i] + frhs1[i] * 7.0 / 27.0 + ft2[i] * 10.0 / 27.0 + ft4[i] / 27.0;
-        dgvo_spatial_oper(c, t0, ft2, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft2, dt, kappa, nthreads);
         for (i = 0; i < N; i++)
             t0[i] = f[i] + frhs1[i] * 28.0 / 625.0 + ft3[i] + ft4[i] * 54 / 625.0 - ft2[i] * 378 / 625.0;
-        dgvo_spatial_oper(c, t0, ft3, dt, kappa, nthreads);
+        dgvo_spatial_oper_regime(c, reg, t0, ft3, dt, kappa, nthreads);
         for (i = 0; i < N; i++)
             f[i] = f[i] + frhs1[i] / 24.0 + ft4[i] * 5.0 / 48.0 + ft2[i] * 27.0 / 56.0 + ft3[i] * 125 / 336.0;
         break;

@@ -85,6 +85,15 @@ void dgvo_eval_linear(const dgvo_ctx *c, const double *fmA, const double *f, dou
 void dgvo_vjp(const dgvo_ctx *c, const double *f, const double *v, double *g, int nthreads);
 
 /* SpatialOperSH_DGV, run_mode 0 (spat_oper_mod.f90:28-68): fcol = Q * kappa * dt */
+/* SpatialOperSH_DGV with CheckSolutionMode_DGV's run modes (spat_oper_mod.f90:28-68, 195-272) */
+typedef struct dgvo_regime dgvo_regime;
+dgvo_regime *dgvo_regime_create(const dgvo_ctx *c, double decomp_lev, double linear_lev);
+void dgvo_regime_free(dgvo_regime *r);
+int dgvo_regime_mode(const dgvo_regime *r, double *last_L1);
+void dgvo_spatial_oper_regime(const dgvo_ctx *c, dgvo_regime *r, const double *f, double *fcol, double dt,
+                              double kappa, int nthreads);
+int dgvo_rk_step_regime(const dgvo_ctx *c, dgvo_regime *r, int order, double *f, double *frhs1, double dt,
+                        double kappa, int nthreads);
 void dgvo_spatial_oper(const dgvo_ctx *c, const double *f, double *fcol, double dt,
                        double kappa, int nthreads);
 /* TimeIntegratorORK_SH_DGV (time_integr_mod.f90:26-152): one step of RK1..RK5.

@@ -69,6 +69,14 @@ def lib():
         L.dgvo_eval_linear.argtypes = [vp, _dp, _dp, _dp]
         L.dgvo_vjp.argtypes = [vp, _dp, _dp, _dp, C.c_int]
         L.dgvo_spatial_oper.argtypes = [vp, _dp, _dp, C.c_double, C.c_double, C.c_int]
+        L.dgvo_regime_create.restype = vp
+        L.dgvo_regime_create.argtypes = [vp, C.c_double, C.c_double]
+        L.dgvo_regime_free.argtypes = [vp]
+        L.dgvo_regime_mode.restype = C.c_int
+        L.dgvo_regime_mode.argtypes = [vp, C.POINTER(C.c_double)]
+        L.dgvo_spatial_oper_regime.argtypes = [vp, vp, _dp, _dp, C.c_double, C.c_double, C.c_int]
+        L.dgvo_rk_step_regime.restype = C.c_int
+        L.dgvo_rk_step_regime.argtypes = [vp, vp, C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int]
         L.dgvo_rk_step.restype = C.c_int
         L.dgvo_rk_step.argtypes = [vp, C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int]
         L.dgvo_ab_step.restype = C.c_int
@@ -246,6 +254,24 @@ class Oracle:
             raise ValueError("bad order")
         return f, frhs1
 
+    # --- run modes of SpatialOperSH_DGV (spat_oper_mod.f90:28-68, 195-272) ----
+    def regime(self, decomp_lev, linear_lev):
+        """A run-mode state (CheckSolutionMode_DGV); pass it to spatial_oper_regime / rk_step_regime."""
+        return _Regime(self, decomp_lev, linear_lev)
+
+    def spatial_oper_regime(self, reg, f, dt, kappa=1.0, nthreads=0):
+        fcol = np.zeros(self.N)
+        lib().dgvo_spatial_oper_regime(self._h, reg._h, np.ascontiguousarray(f, np.float64), fcol, dt, kappa,
+                                       nthreads)
+        return fcol
+
+    def rk_step_regime(self, reg, f, dt, order, kappa=1.0, nthreads=0):
+        f = np.array(f, np.float64, copy=True)
+        frhs1 = np.zeros(self.N)
+        if lib().dgvo_rk_step_regime(self._h, reg._h, order, f, frhs1, dt, kappa, nthreads):
+            raise ValueError("bad order")
+        return f, frhs1
+
     def prepare_ab(self, f, dt, order, kappa=1.0, nthreads=0):
         f = np.array(f, np.float64, copy=True)
         frhs = np.zeros(5 * self.N)
@@ -279,3 +305,23 @@ class Oracle:
 
 def synth_value(seed, p, i2, i3, w2, w3, dsph):
     return lib().dgvo_synth_value(seed, p, i2, i3, w2, w3, dsph)
+
+
+class _Regime:
+    def __init__(self, o, decomp_lev, linear_lev):
+        self._h = lib().dgvo_regime_create(o._h, decomp_lev, linear_lev)
+
+    @property
+    def mode(self):
+        return lib().dgvo_regime_mode(self._h, None)
+
+    @property
+    def last_L1(self):
+        x = C.c_double()
+        lib().dgvo_regime_mode(self._h, C.byref(x))
+        return x.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().dgvo_regime_free(self._h)
+            self._h = None
