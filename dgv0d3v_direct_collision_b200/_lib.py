@@ -27,6 +27,7 @@ EXPORTS = [
     "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
     "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
     "dgv_compute_A", "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
+    "dgv_write_solution", "dgv_read_solution", "dgv_write_solution_arrays", "dgv_read_solution_arrays",
 ]
 
 
@@ -85,6 +86,10 @@ def load() -> C.CDLL:
         "dgv_step_rk": [vp, vp, vp, dbl, C.c_int, C.c_int],
         "dgv_prepare_ab": [vp, vp, dbl, C.c_int, C.c_int],
         "dgv_step_ab": [vp, vp, dbl, C.c_int],
+        "dgv_write_solution": [vp, C.c_char_p, vp, dbl, dbl],
+        "dgv_read_solution": [vp, C.c_char_p, vp, C.POINTER(dbl), C.POINTER(dbl)],
+        "dgv_write_solution_arrays": [C.c_char_p, i32, i32, dbl, dbl, vp],
+        "dgv_read_solution_arrays": [C.c_char_p, C.POINTER(i32), C.POINTER(i32), C.POINTER(dbl), C.POINTER(dbl), vp],
         "dgv_moments": [vp, vp, vp],
         "dgv_maxwellian": [vp, dbl, dbl, dbl, dbl, dbl, vp],
         "dgv_project": [vp, vp, i32],

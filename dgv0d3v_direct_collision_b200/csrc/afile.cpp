@@ -14,6 +14,11 @@
 // A chunked operator is a sequence of such files covering increasing ranges
 // of basis nodes; reading adds their A_capphi arrays and concatenates the
 // records in file order, as ReadAarraysChnksDGV does.
+//
+// A solution file (WriteSol_DGV / RestartSolutionDGV, readwrite.f90:1756-1800,
+// 2389-2513) has the records (e_time, dt), (rkmts), (N) and one record with
+// f, f1..f(rkmts-1), frhs1..frhs(rkmts-1): the solution, the previous
+// solutions and right sides (divided by dt) of the multistep method.
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -265,5 +270,137 @@ extern "C" int dgv_write_A_file(dgv_ctx *ctx, const char *path, int64_t max_subr
     std::string e = write_file(path, (int32_t)c->grid.N, nnz, capphi.data(), A.data(), xi.data(), xi1.data(),
                                max_subrecord ? max_subrecord : kMaxSubrecord);
     if (!e.empty()) return set_err(c, DGV_EINVAL, "write_A_file: " + e);
+    return DGV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// solution files
+
+namespace {
+
+// f may live on the host or the device: cudaMemcpyDefault infers the direction
+std::string copy_any(double *dst, const double *src, size_t n)
+{
+    cudaError_t e = cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyDefault);
+    return e == cudaSuccess ? "" : cudaGetErrorString(e);
+}
+
+// records of WriteSol_DGV: (e_time, dt), (rkmts), (N), then the (2 rkmts - 1)
+// arrays of length N given as pieces
+std::string write_sol(const char *path, int32_t N, int32_t rkmts, double e_time, double dt,
+                      const std::vector<Piece> &arrays)
+{
+    if (rkmts < 1 || rkmts > 5) return "rkmts outside 1..5";
+    File fp;
+    fp.fp = fopen(path, "wb");
+    if (!fp.fp) return std::string("cannot create ") + path;
+    const double td[2] = {e_time, dt};
+    const bool ok = write_record(fp.fp, {{td, 16}}, kMaxSubrecord) && write_record(fp.fp, {{&rkmts, 4}}, kMaxSubrecord) &&
+                    write_record(fp.fp, {{&N, 4}}, kMaxSubrecord) && write_record(fp.fp, arrays, kMaxSubrecord);
+    return ok ? "" : std::string("write failed for ") + path;
+}
+
+struct SolFile {
+    double e_time = 0, dt = 0;
+    int32_t rkmts = 0, N = 0;
+    std::vector<unsigned char> arrays;  // f, f1..f(rkmts-1), frhs1..frhs(rkmts-1)
+};
+
+// RestartSolutionDGV's reads (readwrite.f90:2485-2507)
+std::string read_sol(const char *path, SolFile &s)
+{
+    File fp;
+    fp.fp = fopen(path, "rb");
+    if (!fp.fp) return std::string("cannot open ") + path;
+    std::vector<unsigned char> r1, r2, r3;
+    std::string e = read_record(fp.fp, r1);
+    if (e.empty()) e = read_record(fp.fp, r2);
+    if (e.empty()) e = read_record(fp.fp, r3);
+    if (e.empty()) e = read_record(fp.fp, s.arrays);
+    if (!e.empty()) return e;
+    if (r1.size() != 16 || r2.size() != 4 || r3.size() != 4) return "header records are not (e_time, dt), (rkmts), (N)";
+    double td[2];
+    std::memcpy(td, r1.data(), 16);
+    std::memcpy(&s.rkmts, r2.data(), 4);
+    std::memcpy(&s.N, r3.data(), 4);
+    s.e_time = td[0];
+    s.dt = td[1];
+    if (s.rkmts < 1 || s.rkmts > 5) return "rkmts outside 1..5";
+    if (s.N < 0) return "negative array length";
+    if (s.arrays.size() != (size_t)(2 * s.rkmts - 1) * (size_t)s.N * sizeof(double))
+        return "solution record length is not (2 rkmts - 1) N doubles";
+    return "";
+}
+
+}  // namespace
+
+extern "C" int dgv_write_solution_arrays(const char *path, int32_t N, int32_t rkmts, double e_time, double dt,
+                                         const double *arrays)
+{
+    if (!path || N < 0 || (N > 0 && !arrays)) {
+        g_file_err = "write_solution_arrays: bad arguments";
+        return DGV_EINVAL;
+    }
+    g_file_err = write_sol(path, N, rkmts, e_time, dt, {{arrays, (size_t)(2 * rkmts - 1) * (size_t)N * sizeof(double)}});
+    return g_file_err.empty() ? DGV_OK : DGV_EINVAL;
+}
+
+extern "C" int dgv_read_solution_arrays(const char *path, int32_t *N, int32_t *rkmts, double *e_time, double *dt,
+                                        double *arrays)
+{
+    SolFile s;
+    g_file_err = path ? read_sol(path, s) : "read_solution_arrays: NULL path";
+    if (!g_file_err.empty()) return DGV_EINVAL;
+    if (N) *N = s.N;
+    if (rkmts) *rkmts = s.rkmts;
+    if (e_time) *e_time = s.e_time;
+    if (dt) *dt = s.dt;
+    if (arrays) std::memcpy(arrays, s.arrays.data(), s.arrays.size());
+    return DGV_OK;
+}
+
+extern "C" int dgv_write_solution(dgv_ctx *ctx, const char *path, const double *f, double e_time, double dt)
+{
+    if (!ctx) return DGV_EINVAL;
+    Ctx *c = &ctx->c;
+    if (!path || !f) return set_err(c, DGV_EINVAL, "write_solution: NULL argument");
+    DGV_CUDA(c, cudaSetDevice(c->device));
+    const size_t N = (size_t)c->grid.N;
+    int order = 0;
+    std::vector<double> frhs;
+    int rc = ab_history_get(c, &order, frhs);
+    if (rc) return rc;
+    // before dgv_prepare_ab there is no multistep history: rkmts = 1
+    const int rkmts = order > 0 ? order : 1;
+    // f1..f4 are written as zeros: the multistep formulas never read them
+    std::vector<double> fh(N), prev((size_t)(rkmts - 1) * N, 0.0);
+    std::string e = copy_any(fh.data(), f, N);
+    if (!e.empty()) return set_err(c, DGV_ECUDA, "write_solution: " + e);
+    e = write_sol(path, (int32_t)N, rkmts, e_time, dt,
+                  {{fh.data(), N * sizeof(double)},
+                   {prev.data(), prev.size() * sizeof(double)},
+                   {frhs.data(), frhs.size() * sizeof(double)}});
+    if (!e.empty()) return set_err(c, DGV_EINVAL, "write_solution: " + e);
+    return DGV_OK;
+}
+
+extern "C" int dgv_read_solution(dgv_ctx *ctx, const char *path, double *f, double *e_time, double *dt)
+{
+    if (!ctx) return DGV_EINVAL;
+    Ctx *c = &ctx->c;
+    if (!path || !f) return set_err(c, DGV_EINVAL, "read_solution: NULL argument");
+    DGV_CUDA(c, cudaSetDevice(c->device));
+    SolFile s;
+    std::string e = read_sol(path, s);
+    if (!e.empty()) return set_err(c, DGV_EINVAL, std::string("read_solution: ") + path + ": " + e);
+    const size_t N = (size_t)c->grid.N;
+    if ((size_t)s.N != N) return set_err(c, DGV_EINVAL, "read_solution: array length differs from the grid's N");
+    const double *arr = reinterpret_cast<const double *>(s.arrays.data());
+    e = copy_any(f, arr, N);
+    if (!e.empty()) return set_err(c, DGV_ECUDA, "read_solution: " + e);
+    int rc = ab_history_set(c, s.rkmts, arr + (size_t)s.rkmts * N);  // after f, f1..f(rkmts-1)
+    if (rc) return rc;
+    if (e_time) *e_time = s.e_time;
+    if (dt) *dt = s.dt;
     return DGV_OK;
 }

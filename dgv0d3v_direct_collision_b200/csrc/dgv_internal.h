@@ -177,6 +177,8 @@ int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, i
 int spatial_device(Ctx *c, const double *d_f, double *d_out, double dt, int precision);
 int ab_prepare_device(Ctx *c, double *d_f, double dt, int order, int precision);
 int ab_step_device(Ctx *c, double *d_f, double dt, int precision);
+int ab_history_get(Ctx *c, int *order, std::vector<double> &frhs);
+int ab_history_set(Ctx *c, int order, const double *frhs);
 
 }  // namespace dgv
 

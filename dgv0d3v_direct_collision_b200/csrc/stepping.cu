@@ -512,6 +512,35 @@ int ab_prepare_device(Ctx *c, double *d_f, double dt, int order, int precision)
     return DGV_OK;
 }
 
+// The multistep state a solution file keeps (WriteSol_DGV,
+// readwrite.f90:1756-1800): the method order and frhs1..frhs(order-1),
+// already divided by dt, newest first; host copies.
+int ab_history_get(Ctx *c, int *order, std::vector<double> &frhs)
+{
+    *order = c->ab_order;
+    const size_t N = (size_t)c->grid.N;
+    frhs.assign(c->ab_order > 1 ? (size_t)(c->ab_order - 1) * N : 0, 0.0);
+    for (int j = 0; j + 1 < c->ab_order; j++)
+        DGV_CUDA(c, cudaMemcpyAsync(frhs.data() + (size_t)j * N, c->d_hist[j], N * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->stream));
+    DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DGV_OK;
+}
+
+int ab_history_set(Ctx *c, int order, const double *frhs)
+{
+    if (order < 1 || order > 5) return set_err(c, DGV_EINVAL, "solution file: method order outside 1..5");
+    TRY(ensure_tmp(c));
+    TRY(ensure_hist(c));
+    const size_t N = (size_t)c->grid.N;
+    for (int j = 0; j + 1 < order; j++)
+        DGV_CUDA(c, cudaMemcpyAsync(c->d_hist[j], frhs + (size_t)j * N, N * sizeof(double), cudaMemcpyHostToDevice,
+                                    c->stream));
+    DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->ab_order = order;
+    return DGV_OK;
+}
+
 int ab_step_device(Ctx *c, double *d_f, double dt, int precision)
 {
     int order = c->ab_order;

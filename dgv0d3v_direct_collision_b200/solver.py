@@ -290,6 +290,25 @@ class DGVSolver:
         _check_f64(f)
         self._check(self._lib.dgv_step_ab(self._h, _ptr(f), dt, self._prec(precision)))
 
+    def WriteSol_DGV(self, path: str, f, e_time: float, dt: float):
+        """Write f and the Adams-Bashforth history in the reference's solution
+        file format (WriteSol_DGV; name it with afile.solution_file_name)."""
+        _check_f64(f)
+        self._check(self._lib.dgv_write_solution(self._h, path.encode(), _ptr(f), float(e_time), float(dt)))
+
+    def RestartSolutionDGV(self, path: str, f=None):
+        """Read a solution file into f (a new host array when None) and the
+        Adams-Bashforth history; returns (f, e_time, dt).  rkmts becomes the
+        file's order, as RestartSolutionDGV sets it."""
+        f = np.zeros(self.N) if f is None else f
+        _check_f64(f)
+        t = C.c_double(); dt = C.c_double()
+        self._check(self._lib.dgv_read_solution(self._h, path.encode(), _ptr(f), C.byref(t), C.byref(dt)))
+        r = C.c_int32()
+        if self._lib.dgv_read_solution_arrays(path.encode(), None, C.byref(r), None, None, None) == 0:
+            self.rkmts = r.value
+        return f, t.value, dt.value
+
     # -- moments and equilibrium ----------------------------------------------
     def MassCheckRec(self, f):
         _check_f64(f)

@@ -214,6 +214,27 @@ int dgv_prepare_ab(dgv_ctx *ctx, double *f, double dt, int order, int precision)
 /* One Adams-Bashforth step of the order given to dgv_prepare_ab
  * (TimeIntegratorMTS_SH_DGV, time_integr_mod.f90:314-364). */
 int dgv_step_ab(dgv_ctx *ctx, double *f, double dt, int precision);
+/* Writes a solution file (WriteSol_DGV, readwrite.f90:1756-1796): Fortran
+ * unformatted sequential records (e_time, dt), (rkmts), (N) and
+ * (f, f1..f(rkmts-1), frhs1..frhs(rkmts-1)), rkmts = the order given to
+ * dgv_prepare_ab (1 before it), frhs* = the context's Adams-Bashforth right
+ * sides.  f1..f4 are written as zeros: the multistep formulas never read
+ * them.  f may be a host or a device pointer. */
+int dgv_write_solution(dgv_ctx *ctx, const char *path, const double *f, double e_time, double dt);
+/* Reads such a file (RestartSolutionDGV, readwrite.f90:2389-2513) into f
+ * (host or device) and the context's Adams-Bashforth history, so that
+ * dgv_step_ab continues with order rkmts; e_time / dt may be NULL.  A file
+ * whose N differs from the grid's is refused, as the reference refuses it. */
+int dgv_read_solution(dgv_ctx *ctx, const char *path, double *f, double *e_time, double *dt);
+/* The same solution files without a context or a GPU (WriteSol_DGV,
+ * readwrite.f90:1756-1796): arrays holds f, f1..f(rkmts-1),
+ * frhs1..frhs(rkmts-1), (2 rkmts - 1) N doubles.  Errors: dgv_file_error(). */
+int dgv_write_solution_arrays(const char *path, int32_t N, int32_t rkmts, double e_time, double dt,
+                              const double *arrays);
+/* (RestartSolutionDGV, readwrite.f90:2485-2507) any output may be NULL;
+ * call with arrays = NULL first to learn N and rkmts. */
+int dgv_read_solution_arrays(const char *path, int32_t *N, int32_t *rkmts, double *e_time, double *dt,
+                             double *arrays);
 
 /* -- moments, equilibrium, conservation ----------------------------------- */
 /* out = n, ubar, vbar, wbar, T (MassCheckRec, dgvtools_mod.f90:1437-1458) */
