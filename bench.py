@@ -351,6 +351,66 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line))
 
 
+def run_mixed(args):
+    """Mixed-grid batch: 768 VDFs on the 21^3 grid (s=3, M=7, [-6,6]^3) and
+    256 on the 15^3 grid (s=3, M=5, [-6,6]^3), tensor-core path, evaluated per
+    step by one dgv_collide_group call (one CUDA graph over both contexts'
+    streams).  Timed beside it: the same work as two separate batched calls.
+    Prints its own JSON line (not the headline)."""
+    import torch
+
+    import dgv0d3v_direct_collision_b200 as dgv
+    parts = [(3, 7, 6.0, 768), (3, 5, 6.0, 256)]
+    members = []
+    for i, (s_, m_, l_, nb) in enumerate(parts):
+        sol = dgv.DGVSolver(s_, m_, l_)
+        sol.generate_synthetic_A(seed=SEED_A + i, support=1)
+        fb = mixture_batch(sol.nodes_u, sol.nodes_v, sol.nodes_w, sol.nodes_gwts, nb, 77 + i)
+        f = torch.tensor(fb, dtype=torch.float64, device="cuda")
+        members.append((sol, f, torch.empty_like(f)))
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, clk.summary()
+
+    def group():
+        dgv.collide_group(members, precision="tc", stream_ptr=stream.cuda_stream)
+
+    def separate():
+        for sol, f, q in members:
+            sol.set_stream(stream.cuda_stream)
+            sol.EvalCollisionPeriodicAPlus_DGV(f, q, precision="tc")
+
+    for sol, _, _ in members:
+        sol.kernel_stats(reset=True)
+    ms_g, clk = timed(group)
+    launches = sum(m[0].kernel_stats(reset=True)["all_launches"] for m in members)
+    q_group = [m[2].clone() for m in members]
+    ms_s, _ = timed(separate)
+    same = all(torch.equal(a, m[2]) for a, m in zip(q_group, members))
+    nvdf = sum(p[3] for p in parts)
+    print(json.dumps({
+        "metric": "mixed-grid batch Q(f,f) evals/s (768 x 21^3 + 256 x 15^3, one graph launch per step)",
+        "value": nvdf / (ms_g / 1000.0), "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_g, "higher_is_better": True, "dtype": "f16 hi+lo split products, f32 accumulate, f64 sums",
+        "data": "synthetic",
+        "config": {"workload": "768 VDFs on s=3,M=7,[-6,6]^3 + 256 VDFs on s=3,M=5,[-6,6]^3, tensor-core path",
+                   "A": [m[0].A_info() for m in members],
+                   "l2": "inputs larger than L2: A chunk records of both grids streamed every step"},
+        "separate_calls_ms_per_step": ms_s, "group_over_separate": ms_s / ms_g,
+        "group_equals_separate": bool(same), "gpu_launches": int(launches), "clocks": clk}))
+
+
 def run_profile_case(case: str):
     """Cases for profiler captures.  "<prec>_21": the 21^3 grid (s=3, M=7,
     [-6,6]^3; A rows ~5.6 GB in total) -- one VDF with a fixed chunk count (no
@@ -394,11 +454,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--f64-vdfs", type=int, default=32,
                     help="VDFs of the batch the plain FP64 arm is timed on")
+    ap.add_argument("--mixed", action="store_true",
+                    help="time the mixed-grid batch (768 x 21^3 + 256 x 15^3) instead of the headline")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.profile_case:
         run_profile_case(args.profile_case)
+        return
+    if args.mixed:
+        run_mixed(args)
         return
     if args.impl == "reference":
         # the CPU reference runs on rank 0 only; other ranks exit without work

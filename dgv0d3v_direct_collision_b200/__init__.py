@@ -5,8 +5,8 @@ include/dgv_b200.h); this package is its host-side mirror.  Importing the
 package loads the library and raises if it has not been built.
 """
 from ._lib import DGVError, load as _load
-from .solver import DGVSolver
+from .solver import DGVSolver, collide_group
 
 _load()
 
-__all__ = ["DGVSolver", "DGVError"]
+__all__ = ["DGVSolver", "DGVError", "collide_group"]

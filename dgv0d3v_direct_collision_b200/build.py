@@ -34,6 +34,7 @@ SOURCES = [
     ("synth.cu", ["-fmad=false"]),
     ("seta.cu", ["-fmad=false"]),
     ("stepping.cu", ["-fmad=false"]),
+    ("group.cu", []),
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -74,6 +74,8 @@ static bool is_device_ptr(const void *p)
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
+bool is_device_pointer(const void *p) { return is_device_ptr(p); }
+
 // Inverse of the Gram matrix G_ab = sum_i w_i psi_a psi_b of the invariants
 static int gram_inverse(Ctx *c)
 {

@@ -430,12 +430,16 @@ struct RkGraphKey {
 struct RkGraph {
     int calls = 0;
     cudaGraphExec_t exec = nullptr;
+    long long launches = 0;  // kernels in the graph, counted while capturing
 };
 static std::map<const Ctx *, std::map<RkGraphKey, RkGraph>> g_graphs;
 static std::recursive_mutex g_graphs_mu;  // contexts on different host threads share the cache
 
+void release_group_graphs(const Ctx *c);
+
 void release_graphs(const Ctx *c)
 {
+    release_group_graphs(c);
     std::lock_guard<std::recursive_mutex> lk(g_graphs_mu);
     auto it = g_graphs.find(c);
     if (it == g_graphs.end()) return;
@@ -459,19 +463,28 @@ int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, i
     RkGraph &gr = g_graphs[c][key];
     if (gr.exec) {
         DGV_CUDA(c, cudaGraphLaunch(gr.exec, c->stream));
+        count_launches(c, gr.launches);
         return DGV_OK;
     }
     if (gr.calls++ == 0) return rk_body(c, d_f, r1, dt, order, precision);
+    const long long before = c->kt_all;
     cudaGraph_t graph = nullptr;
     DGV_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = rk_body(c, d_f, r1, dt, order, precision);
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
     if (e != cudaSuccess) return set_err(c, DGV_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return set_err(c, DGV_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-    DGV_CUDA(c, cudaGraphLaunch(gr.exec, c->stream));
+    // looked up again: a buffer that grew while capturing released the cache
+    RkGraph &g2 = g_graphs[c][key];
+    if (g2.exec) cudaGraphExecDestroy(g2.exec);
+    g2.exec = exec;
+    g2.calls = 2;
+    g2.launches = c->kt_all - before;
+    DGV_CUDA(c, cudaGraphLaunch(exec, c->stream));
     return DGV_OK;
 }
 

@@ -320,3 +320,24 @@ class DGVSolver:
         out = np.zeros(self.N) if out is None else out
         self._check(self._lib.dgv_maxwellian(self._h, T, u0, v0, w0, n, _ptr(out)))
         return out
+
+
+def collide_group(members, precision: Optional[str] = None, stream_ptr: int = 0):
+    """Q of a mixed batch over several grids in one call: members is a list
+    of (solver, f, q) with f, q device tensors [nb, N] of that solver's grid
+    (all solvers on one device).  Repeated calls with the same members replay
+    one captured CUDA graph (dgv_collide_group)."""
+    if not members:
+        raise ValueError("need at least one member")
+    n = len(members)
+    s0 = members[0][0]
+    ctxs = (C.c_void_p * n)(*[m[0]._h.value for m in members])
+    nbs, fs, qs = (C.c_int32 * n)(), (C.c_void_p * n)(), (C.c_void_p * n)()
+    for i, (s, f, q) in enumerate(members):
+        _check_f64(f); _check_f64(q)
+        nb = int(np.prod(f.shape)) // s.N
+        if nb < 1 or nb * s.N != int(np.prod(f.shape)) or int(np.prod(q.shape)) != nb * s.N:
+            raise ValueError(f"member {i}: f and q must hold nb x {s.N} values")
+        nbs[i], fs[i], qs[i] = nb, _ptr(f), _ptr(q)
+    s0._check(s0._lib.dgv_collide_group(n, ctxs, nbs, fs, qs, s0._prec(precision), stream_ptr or None))
+    return [m[2] for m in members]

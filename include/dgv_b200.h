@@ -162,6 +162,17 @@ const char *dgv_file_error(void);
 int dgv_collide(dgv_ctx *ctx, const double *f, double *q, int64_t n, int precision);
 /* nb VDFs stored contiguously, f[nb][N] -> q[nb][N] */
 int dgv_collide_batched(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int precision);
+/* One mixed batch over n velocity grids (one context per grid, all on one
+ * device): q[k][nb[k]][N_k] = Q(f[k]) on ctxs[k]'s grid, device pointers
+ * only.  The members run on their contexts' streams, forked from and joined
+ * back to `stream` (NULL = ctxs[0]'s stream).  The first call for a member
+ * list runs eagerly, the second captures the group in one CUDA graph, later
+ * calls replay it with one launch; a context whose buffers or A-arrays change
+ * drops the graphs it belongs to.  Errors are reported on ctxs[0].  The
+ * reference evaluates each VDF with EvalCollisionPeriodicAPlus_DGV
+ * (collision_mod.f90:143-229) on one grid per run. */
+int dgv_collide_group(int32_t n, dgv_ctx *const *ctxs, const int32_t *nb, const double *const *f,
+                      double *const *q, int precision, void *stream);
 /* fcol = kappa*dt*Q(f,f) (SpatialOperSH_DGV, spat_oper_mod.f90:28-68); with
  * run modes switched on (dgv_set_regime) the mode of CheckSolutionMode_DGV
  * decides: Q(f), L(Df) + Q(Df) or L(Df), Df = f - fm */

@@ -76,7 +76,7 @@ def test_restart_into_device_memory_and_errors(golden, tmp_path):
     assert rel_err(gd.cpu().numpy(), fd.cpu().numpy()) < TOL64
 
     # a file of another grid is refused, as RestartSolutionDGV refuses m /= size(f,1)
-    other = dgv.DGVSolver(2, 3, 3.0)
+    other = dgv.DGVSolver(2, 4, 4.0)  # N = 512, the golden grid has 216
     with pytest.raises(dgv.DGVError):
         other.RestartSolutionDGV(path)
     with pytest.raises(dgv.DGVError):
