@@ -2,7 +2,7 @@
 each, evaluated through one fork/join over the contexts' streams -- eager
 first call, captured second call, replays after -- against separate calls and
 the oracle (FP64 <= 1e-12, tensor cores <= 1e-6 norm-wise per VDF), replays
-following new input values, and launch counts of a replay equal to the eager
+following new input values, and launch counts of a replay equal to an eager
 call's."""
 import numpy as np
 import pytest
@@ -63,7 +63,8 @@ def test_group_matches_oracle_and_replays(grids, precision, tol):
             sol.kernel_stats(reset=True)  # drop the separate call's launches
     for sol in (m[0] for m in members):
         sol.set_kernel_timing(False)
-    assert counts[0] == counts[1] == counts[2] == counts[3] and min(counts[0]) > 0
+    # the first call also runs the chunk-count tuning launches
+    assert counts[1] == counts[2] == counts[3] and min(counts[1]) > 0
 
 
 def test_group_rejects_host_arrays(grids):
