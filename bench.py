@@ -353,7 +353,8 @@ def run_ours(args, world, rank, local):
 
 def run_mixed(args):
     """Mixed-grid batch: 768 VDFs on the 21^3 grid (s=3, M=7, [-6,6]^3) and
-    256 on the 15^3 grid (s=3, M=5, [-6,6]^3), tensor-core path, evaluated per
+    256 on the 15^3 grid (s=3, M=5, [-6,6]^3), seeded Maxwellian mixtures times
+    (1 + 0.1 N(0,1)) per node clipped at 0, tensor-core path, evaluated per
     step by one dgv_collide_group call (one CUDA graph over both contexts'
     streams).  Timed beside it: the same work as two separate batched calls.
     Prints its own JSON line (not the headline)."""
@@ -366,6 +367,8 @@ def run_mixed(args):
         sol = dgv.DGVSolver(s_, m_, l_)
         sol.generate_synthetic_A(seed=SEED_A + i, support=1)
         fb = mixture_batch(sol.nodes_u, sol.nodes_v, sol.nodes_w, sol.nodes_gwts, nb, 77 + i)
+        # multiplicative perturbation per node, clipped at 0
+        fb *= np.clip(1.0 + 0.1 * np.random.default_rng(99 + i).standard_normal(fb.shape), 0.0, None)
         f = torch.tensor(fb, dtype=torch.float64, device="cuda")
         members.append((sol, f, torch.empty_like(f)))
     stream = torch.cuda.current_stream()
@@ -409,6 +412,54 @@ def run_mixed(args):
                    "l2": "inputs larger than L2: A chunk records of both grids streamed every step"},
         "separate_calls_ms_per_step": ms_s, "group_over_separate": ms_s / ms_g,
         "group_equals_separate": bool(same), "gpu_launches": int(launches), "clocks": clk}))
+
+
+def run_trajectory(args):
+    """RK4 relaxation on the 21^3 grid (s=3, M=7, [-6,6]^3): a seeded
+    Maxwellian mixture (1-4 components, density 1) advanced 500 steps with
+    dt = 0.005 by the FP32-compensated and the FP64 paths side by side, with
+    the conservation projection.  At every step: the error of the FP32 Q
+    against the FP64 Q on the FP64 state, the distance between the two
+    trajectories, and the drift of the moments of both.  Prints a JSON
+    summary (not the headline)."""
+    import torch
+
+    import dgv0d3v_direct_collision_b200 as dgv
+    kappa, dt, steps = 0.1, 0.005, args.trajectory_steps
+    s = dgv.DGVSolver(3, 7, 6.0, kappa=kappa)
+    s.generate_synthetic_A(seed=SEED_A, support=1)
+    s.set_projection(True)
+    f0 = mixture_batch(s.nodes_u, s.nodes_v, s.nodes_w, s.nodes_gwts, 1, 5)[0]
+    f64 = torch.tensor(f0, device="cuda")
+    f32 = f64.clone()
+    r64, r32 = torch.zeros_like(f64), torch.zeros_like(f64)
+    q64, q32 = torch.zeros_like(f64), torch.zeros_like(f64)
+    m0 = np.array(s.MassCheckRec(f0))
+
+    def rel(x, y):
+        return float(torch.linalg.norm(x - y) / torch.linalg.norm(y))
+
+    qerr, traj, drift = [], [], []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.EvalCollisionPeriodicAPlus_DGV(f64, q64, precision="f64")
+        s.EvalCollisionPeriodicAPlus_DGV(f64, q32, precision="f32c")
+        qerr.append(rel(q32, q64))
+        s.TimeIntegratorORK_SH_DGV(f64, dt, frhs1=r64, order=4, precision="f64")
+        s.TimeIntegratorORK_SH_DGV(f32, dt, frhs1=r32, order=4, precision="f32c")
+        traj.append(rel(f32, f64))
+        m64, m32 = np.array(s.MassCheckRec(f64)), np.array(s.MassCheckRec(f32))
+        drift.append(float(max(np.max(np.abs(m64 - m0) / np.maximum(1.0, np.abs(m0))),
+                               np.max(np.abs(m32 - m0) / np.maximum(1.0, np.abs(m0))))))
+    wall = time.perf_counter() - t0
+    print(json.dumps({
+        "case": "RK4 relaxation, 21^3 (s=3, M=7, [-6,6]^3), FP32-compensated vs FP64, projection on",
+        "steps": steps, "dt": dt, "kappa": kappa, "A": s.A_info(),
+        "q_err_f32c_vs_f64": {"max": max(qerr), "median": float(np.median(qerr)), "last": qerr[-1]},
+        "trajectory_distance": {"max": max(traj), "last": traj[-1]},
+        "moment_drift_max": max(drift),
+        "state_change": float(torch.linalg.norm(f64 - torch.tensor(f0, device="cuda")) / np.linalg.norm(f0)),
+        "wall_s": wall}))
 
 
 def run_profile_case(case: str):
@@ -456,6 +507,9 @@ def main():
                     help="VDFs of the batch the plain FP64 arm is timed on")
     ap.add_argument("--mixed", action="store_true",
                     help="time the mixed-grid batch (768 x 21^3 + 256 x 15^3) instead of the headline")
+    ap.add_argument("--trajectory", action="store_true",
+                    help="RK4 relaxation at 21^3, FP32-compensated vs FP64 per step (report, not the headline)")
+    ap.add_argument("--trajectory-steps", type=int, default=500)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -464,6 +518,9 @@ def main():
         return
     if args.mixed:
         run_mixed(args)
+        return
+    if args.trajectory:
+        run_trajectory(args)
         return
     if args.impl == "reference":
         # the CPU reference runs on rank 0 only; other ranks exit without work
