@@ -220,6 +220,8 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.Stream()
     solver = dgv.DGVSolver(S, M, L, device=local)
     solver.set_stream(stream.cuda_stream)
+    if args.tc_form:
+        solver.set_tc_form(args.tc_form)
     t = time.perf_counter()
     solver.generate_synthetic_A(seed=SEED_A, support=1)
     t_gen = time.perf_counter() - t
@@ -475,6 +477,9 @@ def run_profile_case(case: str):
     prec, grid = case.split("_")
     s = dgv.DGVSolver(S, M, L) if grid == "27" else dgv.DGVSolver(3, 7, 6.0)
     s.generate_synthetic_A(seed=SEED_A, support=1)
+    if prec == "tc2":
+        s.set_tc_form(2)
+        prec = "tc"
     if prec != "tc":
         s.set_nchunks(296)
     nb = BATCH if prec == "tc" else 1
@@ -495,7 +500,8 @@ def run_profile_case(case: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21", "tc_27"], default=None,
+    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21", "tc_27", "tc2_21", "tc2_27"],
+                    default=None,
                     help="small single-VDF case for profiler captures (no JSON bench line)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -510,6 +516,8 @@ def main():
     ap.add_argument("--trajectory", action="store_true",
                     help="RK4 relaxation at 21^3, FP32-compensated vs FP64 per step (report, not the headline)")
     ap.add_argument("--trajectory-steps", type=int, default=500)
+    ap.add_argument("--tc-form", type=int, default=0, choices=[0, 1, 2],
+                    help="tensor-core form of the headline arm (0 = the library default)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -574,14 +574,12 @@ __global__ void k_tc_final(const double *qacc, const double *w, double *q, long 
 }
 
 // ----------------------------------------------------------------------------
-static int tc_prepare(Ctx *c)
+// power-of-two scale of the A values: the largest |value| -> [2^13, 2^14), so
+// fp16 hi parts stay finite
+static int tc_value_scale(Ctx *c, double *scale)
 {
-    Layout &L = c->lay;
-    if (L.tc_V) return DGV_OK;
+    const Layout &L = c->lay;
     const Grid &g = c->grid;
-    std::vector<int> cs(L.nblocks + 1, 0);
-    for (long long b = 0; b < L.nblocks; b++) cs[b + 1] = cs[b] + (L.h_blk[b].count + TC_KCH - 1) / TC_KCH;
-    const long long nch = cs[L.nblocks];
     unsigned long long *d_max = nullptr;
     DGV_CUDA(c, cudaMalloc(&d_max, sizeof(unsigned long long)));
     DGV_CUDA(c, cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream));
@@ -596,9 +594,22 @@ static int tc_prepare(Ctx *c)
     int e = 0;
     if (vmax > 0.0) {
         std::frexp(vmax, &e);
-        e = 14 - e;  // largest |value| -> [2^13, 2^14): fp16 hi parts stay finite
+        e = 14 - e;
     }
-    L.tc_vscale = std::ldexp(1.0, e);
+    *scale = std::ldexp(1.0, e);
+    return DGV_OK;
+}
+
+static int tc_prepare(Ctx *c)
+{
+    Layout &L = c->lay;
+    if (L.tc_V) return DGV_OK;
+    const Grid &g = c->grid;
+    std::vector<int> cs(L.nblocks + 1, 0);
+    for (long long b = 0; b < L.nblocks; b++) cs[b + 1] = cs[b] + (L.h_blk[b].count + TC_KCH - 1) / TC_KCH;
+    const long long nch = cs[L.nblocks];
+    int rc = tc_value_scale(c, &L.tc_vscale);
+    if (rc) return rc;
     DGV_CUDA(c, cudaMalloc(&L.tc_chunk_start, sizeof(int) * (L.nblocks + 1)));
     DGV_CUDA(c, cudaMemcpy(L.tc_chunk_start, cs.data(), sizeof(int) * (L.nblocks + 1), cudaMemcpyHostToDevice));
     DGV_CUDA(c, cudaMalloc(&L.tc_V, (size_t)std::max<long long>(1, nch) * TC_REC));
@@ -622,21 +633,23 @@ static int tc_prepare(Ctx *c)
     return DGV_OK;
 }
 
-// Work lists, built once per cells-per-tile NDG: for every launch (block
-// set) and row tile (NDG consecutive output cells), the blocks whose valid
-// box meets the tile, in block order, with the tile cells each is valid for.
-// Tiles of a launch are ordered by the chunk records they consume, heaviest
-// first, so the last wave of CTAs is short.
+// Work lists, built once per cells-per-tile NDG and form: for every launch
+// (block set) and row tile (NDG consecutive output cells), the blocks whose
+// valid box meets the tile, in block order, with the tile cells each is valid
+// for.  Tiles of a launch are ordered by their work, heaviest first, so the
+// last wave of CTAs is short.  An item carries first[b] (the block's first
+// chunk record, or the block index) and count[b] (its chunk records, or 1).
 struct TcLists {
     TcItem *items = nullptr;
     int *item_start = nullptr;  // per set: ntiles + 1 entries
     int *tile_of = nullptr;     // per set: ntiles entries
 };
 
-static int tc_lists(Ctx *c, int NDG, TcLists *out)
+static int tc_work_lists(Ctx *c, int NDG, int key, const std::vector<int> &sets, const std::vector<int> &first,
+                         const std::vector<int> &count, TcLists *out)
 {
     Layout &L = c->lay;
-    auto it = L.tc_lists.find(NDG);
+    auto it = L.tc_lists.find(key);
     if (it != L.tc_lists.end()) {
         out->items = reinterpret_cast<TcItem *>(it->second[0]);
         out->item_start = reinterpret_cast<int *>(it->second[1]);
@@ -644,7 +657,7 @@ static int tc_lists(Ctx *c, int NDG, TcLists *out)
         return DGV_OK;
     }
     const Grid &g = c->grid;
-    const int ng = (g.Nc + NDG - 1) / NDG, nsets = (int)L.tc_sets.size() - 1;
+    const int ng = (g.Nc + NDG - 1) / NDG, nsets = (int)sets.size() - 1;
     std::vector<TcItem> items;
     std::vector<int> start((size_t)nsets * (ng + 1)), tile_of((size_t)nsets * ng);
     std::vector<std::vector<TcItem>> per(ng);
@@ -652,18 +665,17 @@ static int tc_lists(Ctx *c, int NDG, TcLists *out)
     for (int s = 0; s < nsets; s++) {
         for (auto &v : per) v.clear();
         std::fill(work.begin(), work.end(), 0);
-        for (int b = L.tc_sets[s]; b < L.tc_sets[s + 1]; b++) {
+        for (int b = sets[s]; b < sets[s + 1]; b++) {
             const BlockInfo &bi = L.h_blk[b];
-            const int ch = L.tc_chunk_host[b + 1] - L.tc_chunk_host[b];
             int last = -1;
             for (int u = bi.lo[0]; u <= bi.hi[0]; u++)
                 for (int v = bi.lo[1]; v <= bi.hi[1]; v++)
                     for (int w = bi.lo[2]; w <= bi.hi[2]; w++) {
                         const int D = (u * g.d.Mv + v) * g.d.Mw + w, grp = D / NDG;
                         if (grp != last) {  // cells of one tile are consecutive: same tile as the last cell or new
-                            if (per[grp].empty() || per[grp].back().chunk0 != L.tc_chunk_host[b]) {
-                                per[grp].push_back(TcItem{L.tc_chunk_host[b], ch, bi.c1, bi.c2});
-                                work[grp] += ch;
+                            if (per[grp].empty() || per[grp].back().chunk0 != first[b]) {
+                                per[grp].push_back(TcItem{first[b], count[b], bi.c1, bi.c2});
+                                work[grp] += count[b];
                             }
                             last = grp;
                         }
@@ -688,10 +700,445 @@ static int tc_lists(Ctx *c, int NDG, TcLists *out)
     if (!items.empty()) DGV_CUDA(c, cudaMemcpy(d[0], items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice));
     DGV_CUDA(c, cudaMemcpy(d[1], start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
     DGV_CUDA(c, cudaMemcpy(d[2], tile_of.data(), sizeof(int) * tile_of.size(), cudaMemcpyHostToDevice));
-    L.tc_lists[NDG] = {d[0], d[1], d[2]};
+    L.tc_lists[key] = {d[0], d[1], d[2]};
     out->items = reinterpret_cast<TcItem *>(d[0]);
     out->item_start = reinterpret_cast<int *>(d[1]);
     out->tile_of = reinterpret_cast<int *>(d[2]);
+    return DGV_OK;
+}
+
+static int tc_lists(Ctx *c, int NDG, TcLists *out)
+{
+    const Layout &L = c->lay;
+    std::vector<int> first(L.nblocks), count(L.nblocks);
+    for (long long b = 0; b < L.nblocks; b++) {
+        first[b] = L.tc_chunk_host[b];
+        count[b] = L.tc_chunk_host[b + 1] - L.tc_chunk_host[b];
+    }
+    return tc_work_lists(c, NDG, NDG, L.tc_sets, first, count, out);
+}
+
+// ============================================================================
+// Block form.  The values of a cell-pair block (c1, c2) form a dense matrix
+//   W[l2, (l1, p)] = V[pair (l1, l2), p]   (0 where the block has no pair),
+// so that for output cell D and VDF b
+//   Q[(D,b), p] += sum_l1 f_b(c1+D, l1) * G[(D,b), (l1, p)],   G = F2 W,
+//   F2[(D,b), l2] = f_b(c2+D, l2).
+// G is a tensor-core product per block: M = 128 rows, K = 32 nodes l2
+// (zero-padded), N = P*P columns (l1, p) in groups of 128; F2 and W are split
+// into fp16 hi + lo and hi*hi, hi*lo and lo*hi go into one FP32 accumulator.
+// The CUDA cores then contract each group of G with f(c1+D) in FP32 and add the
+// block total into a (sum, correction) pair with two-sum, in registers.  The
+// per-pair products of the chunk form become columns of G: the CUDA cores do
+// P*P multiply-adds per row and block instead of forming and splitting one
+// product per pair and row.
+//
+// A CTA owns one row tile (NDG output cells x VB VDFs) for two consecutive
+// VDF tiles, so each block's W crosses from L2 once for 256 rows.
+// Warp roles (320 threads, one CTA per SM):
+//   warp 0     producer: TMA bulk copies of f (both tiles) and W groups
+//   warp 1     allocates all 512 tensor-memory columns; lane 0 issues MMAs
+//   warps 2-9  epilogue: warp w serves VDF tile (w-2)/4, tensor-memory lanes
+//              32*(w%4) .. +31 (one row per thread)
+// Tensor memory: four accumulators of 128 columns, used round-robin by the
+// (group, VDF tile) jobs.  Every wait is bounded, as in the chunk form.
+constexpr int T2_N = 128;                     // columns (l1, p) per group
+constexpr int T2_K = 32;                      // nodes l2 per block, zero-padded
+constexpr int T2_TILE = T2_N * T2_K * 2;      // one fp16 tile (8 KiB)
+constexpr int T2_GREC = 2 * T2_TILE;          // hi and lo tiles of one group
+constexpr int T2_NSTW = 4;                    // W ring stages
+constexpr int T2_ATILE = TC_ROWS * T2_K * 2;  // 128 rows x 32 fp16 (8 KiB)
+constexpr int T2_EPI_WARPS = 8;
+constexpr int T2_THREADS = 32 * (2 + T2_EPI_WARPS);
+
+__host__ __device__ constexpr int t2_groups(int P) { return (P * P + T2_N - 1) / T2_N; }
+
+// byte offset of element (row, k) of a K-major tile without swizzle, K = 32:
+// core matrices of 8 rows x 16 bytes, four along K (128 B apart), row groups
+// of 8 512 B apart
+__host__ __device__ __forceinline__ int t2_off(int row, int k)
+{
+    return ((row >> 3) * 4 + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// one record per block: t2_groups(P) groups of {W hi tile, W lo tile}, group
+// g holding columns n = l1*P + p in [128 g, 128 g + 128) as tile rows
+__global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64, int P, int Nc, int ccell,
+                            float vscale, unsigned char *W)
+{
+    const int NG = t2_groups(P);
+    const BlockInfo bi = blk[blockIdx.x];
+    unsigned char *rec = W + (size_t)blockIdx.x * NG * T2_GREC;
+    uint4 *r4 = reinterpret_cast<uint4 *>(rec);
+    for (int t = threadIdx.x; t < NG * T2_GREC / 16; t += blockDim.x) r4[t] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    for (int t = threadIdx.x; t < bi.count * P; t += blockDim.x) {
+        const int k = t / P, p = t - k * P;
+        const double *row = rows64 + (size_t)(bi.start + k) * RD64;
+        const long long o = __double_as_longlong(row[0]);
+        const int o1 = (int)(unsigned)(o & 0xffffffffLL), o2 = (int)(o >> 32);
+        const int l1 = (o1 - (bi.c1 - ccell)) / Nc, l2 = (o2 - (bi.c2 - ccell)) / Nc;
+        const int n = l1 * P + p, g = n / T2_N;
+        const float x = (float)(row[1 + p] * (double)vscale);
+        const __half h = __float2half_rn(x);
+        const __half l = __float2half_rn(x - __half2float(h));
+        unsigned char *dst = rec + (size_t)g * T2_GREC + t2_off(n - g * T2_N, l2);
+        *reinterpret_cast<__half *>(dst) = h;
+        *reinterpret_cast<__half *>(dst + T2_TILE) = l;
+    }
+}
+
+// F16[((bt*2 + h)*Nc + cell) * VB*64 + t2_off(v, l)]: per VDF tile and cell a
+// tile of VB rows (VDFs) x 32 nodes, h = 0 hi / 1 lo parts of the scaled FP32
+// copy F[((bt*Nc + cell)*P + l)*VB + v]; nodes l >= P are zero
+__global__ void k_tc2_f16(const float *F, unsigned char *F16, int nbt, int Nc, int P, int VB)
+{
+    const long long total = (long long)nbt * Nc * T2_K * VB;
+    const size_t tile = (size_t)VB * T2_K * 2;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(i % VB);
+        long long r = i / VB;
+        const int l = (int)(r % T2_K);
+        r /= T2_K;
+        const int cell = (int)(r % Nc), bt = (int)(r / Nc);
+        const float x = l < P ? F[(((size_t)bt * Nc + cell) * P + l) * VB + v] : 0.f;
+        const __half h = __float2half_rn(x);
+        const __half lo = __float2half_rn(x - __half2float(h));
+        unsigned char *base = F16 + ((size_t)(2 * bt) * Nc + cell) * tile + t2_off(v, l);
+        *reinterpret_cast<__half *>(base) = h;
+        *reinterpret_cast<__half *>(base + (size_t)Nc * tile) = lo;
+    }
+}
+
+struct Tc2Args {
+    const float *F;            // [nbt][Nc][P][VB] scaled f, zero for padded VDFs
+    const unsigned char *F16;  // [nbt][hi, lo][Nc][VB x 32 tile]
+    const unsigned char *W;    // block records
+    const TcItem *items;       // work lists of this launch (chunk0 = block index)
+    const int *item_start;     // [ntiles + 1]
+    const int *tile_of;        // row-tile index in launch order
+    double *qacc;              // [(D*P+p)*NV + vdf]
+    const double *inv_scale;   // [NV]
+    int *err;
+    int Nc, ccell, NV, nvdf, nbt, nbp;
+    int region;  // bytes per VDF tile in an item slot: A hi, A lo, f(c1) (FP32)
+};
+
+template <int VB, int P>
+__global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
+{
+    constexpr int NDG = TC_ROWS / VB;
+    constexpr int NG = t2_groups(P);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *wring = smem;                      // T2_NSTW x T2_GREC
+    unsigned char *slots = smem + T2_NSTW * T2_GREC;  // 2 item slots x 2 VDF tiles x region
+    uint64_t *bars = reinterpret_cast<uint64_t *>(slots + 4 * a.region);
+    uint64_t *w_full = bars, *w_empty = bars + T2_NSTW;
+    uint64_t *s_full = w_empty + T2_NSTW, *s_empty = s_full + 2;
+    uint64_t *c_full = s_empty + 2, *c_empty = c_full + 4;
+    uint64_t *drain = c_empty + 4;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bp = blockIdx.x % a.nbp, ti = blockIdx.x / a.nbp;
+    const int bt0 = 2 * bp, nb2 = min(2, a.nbt - bt0);
+    const int D0 = a.tile_of[ti] * NDG;
+    const int i0 = a.item_start[ti], i1 = a.item_start[ti + 1];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < T2_NSTW; s++) {
+            mbar_init(&w_full[s], 1);
+            mbar_init(&w_empty[s], 1);
+        }
+        for (int s = 0; s < 2; s++) {
+            mbar_init(&s_full[s], 1);
+            mbar_init(&s_empty[s], 1 + 4 * nb2);  // the MMA commit + the epilogue warps
+        }
+        for (int s = 0; s < 4; s++) {
+            mbar_init(&c_full[s], 1);
+            mbar_init(&c_empty[s], 4);
+        }
+        mbar_init(drain, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            int q = 0, gw = 0;
+            bool ok = true;
+            const size_t tile = (size_t)VB * T2_K * 2;
+            for (int it = i0; it < i1 && ok; it++) {
+                const TcItem e = a.items[it];
+                const int s = q & 1;
+                if (!mbar_wait(&s_empty[s], ((q >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
+                // f of cells c1 + D - ccell (FP32) and c2 + D - ccell (fp16
+                // tiles), D in the row tile, clipped to the grid
+                const int cs1 = e.c1 + D0 - a.ccell, cs2 = e.c2 + D0 - a.ccell;
+                const int lo1 = max(cs1, 0), hi1 = min(cs1 + NDG, a.Nc);
+                const int lo2 = max(cs2, 0), hi2 = min(cs2 + NDG, a.Nc);
+                uint32_t tx = 0;
+                if (hi1 > lo1) tx += (uint32_t)(nb2 * (hi1 - lo1) * P * VB * 4);
+                if (hi2 > lo2) tx += (uint32_t)(nb2 * 2 * (hi2 - lo2) * tile);
+                if (tx) {
+                    mbar_arrive_expect_tx(&s_full[s], tx);
+                    for (int j = 0; j < nb2; j++) {
+                        const int bt = bt0 + j;
+                        unsigned char *reg = slots + (size_t)(2 * s + j) * a.region;
+                        if (hi2 > lo2) {
+                            const unsigned char *src = a.F16 + ((size_t)(2 * bt) * a.Nc + lo2) * tile;
+                            const uint32_t nb = (uint32_t)((hi2 - lo2) * tile);
+                            bulk_g2s(reg + (lo2 - cs2) * tile, src, nb, &s_full[s]);
+                            bulk_g2s(reg + T2_ATILE + (lo2 - cs2) * tile, src + (size_t)a.Nc * tile, nb, &s_full[s]);
+                        }
+                        if (hi1 > lo1)
+                            bulk_g2s(reg + 2 * T2_ATILE + (size_t)(lo1 - cs1) * P * VB * 4,
+                                     a.F + ((size_t)bt * a.Nc + lo1) * P * VB, (uint32_t)((hi1 - lo1) * P * VB * 4),
+                                     &s_full[s]);
+                    }
+                } else {
+                    mbar_arrive(&s_full[s]);
+                }
+                q++;
+                for (int g = 0; g < NG; g++, gw++) {
+                    const int st = gw % T2_NSTW;
+                    if (!mbar_wait(&w_empty[st], ((gw / T2_NSTW) & 1) ^ 1, a.err)) { ok = false; break; }
+                    mbar_arrive_expect_tx(&w_full[st], T2_GREC);
+                    bulk_g2s(wring + st * T2_GREC, a.W + ((size_t)e.chunk0 * NG + g) * T2_GREC, T2_GREC, &w_full[st]);
+                }
+            }
+            if (!ok) {  // let the copies already issued land
+                for (int j = gw > T2_NSTW ? gw - T2_NSTW : 0; j < gw; j++)
+                    mbar_wait(&w_full[j % T2_NSTW], (j / T2_NSTW) & 1, a.err);
+                for (int j = q > 2 ? q - 2 : 0; j < q; j++) mbar_wait(&s_full[j & 1], (j >> 1) & 1, a.err);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            // FP32 accumulator, fp16 A and B, both K-major, M = 128, N = 128
+            const uint32_t idesc = (1u << 4) | ((uint32_t)(T2_N >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            int q = 0, gw = 0, J = 0;
+            bool ok = true;
+            for (int it = i0; it < i1 && ok; it++) {
+                const int s = q & 1;
+                if (!mbar_wait(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
+                for (int g = 0; g < NG && ok; g++, gw++) {
+                    const int st = gw % T2_NSTW;
+                    if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err)) { ok = false; break; }
+                    const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
+                    const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
+                    for (int j = 0; j < nb2; j++, J++) {
+                        const int cs = J & 3;
+                        if (!mbar_wait(&c_empty[cs], ((J >> 2) & 1) ^ 1, a.err)) { ok = false; break; }
+                        tc_fence_after();
+                        unsigned char *reg = slots + (size_t)(2 * s + j) * a.region;
+                        const uint64_t dAh = umma_desc(smem_u32(reg), 128, 512);
+                        const uint64_t dAl = umma_desc(smem_u32(reg + T2_ATILE), 128, 512);
+                        const uint32_t dacc = tmem + (uint32_t)(cs * T2_N);
+#pragma unroll
+                        for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 256 B along K
+                            umma_f16(dacc, dAh + 16 * t, dWh + 16 * t, idesc, t ? 1u : 0u);
+                            umma_f16(dacc, dAh + 16 * t, dWl + 16 * t, idesc, 1u);
+                            umma_f16(dacc, dAl + 16 * t, dWh + 16 * t, idesc, 1u);
+                        }
+                        umma_commit(&c_full[cs]);
+                    }
+                    if (!ok) break;
+                    umma_commit(&w_empty[st]);
+                }
+                if (!ok) break;
+                umma_commit(&s_empty[s]);
+                q++;
+            }
+            // every MMA issued so far completes before tensor memory is freed
+            umma_commit(drain);
+            mbar_wait(drain, 0, a.err);
+        }
+        __syncwarp();
+    } else if ((warp - 2) / 4 < nb2) {
+        // ---------------- epilogue ----------------
+        const int j = (warp - 2) / 4, quarter = warp & 3, r = quarter * 32 + lane;
+        const uint32_t tl = tmem + ((uint32_t)(quarter * 32) << 16);
+        const int d = r / VB, v = r % VB;
+        float S[P], Cc[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
+        int q = 0;
+        bool ok = true;
+        for (int it = i0; it < i1 && ok; it++) {
+            const bool valid = (a.items[it].nch >> (16 + d)) & 1;
+            const int s = q & 1;
+            if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
+            const float *f1s =
+                reinterpret_cast<const float *>(slots + (size_t)(2 * s + j) * a.region + 2 * T2_ATILE) + d * P * VB + v;
+            float f1[P], acc[P];
+#pragma unroll
+            for (int l = 0; l < P; l++) { f1[l] = f1s[l * VB]; acc[l] = 0.f; }
+#pragma unroll
+            for (int g = 0; g < NG; g++) {
+                const int J = (q * NG + g) * nb2 + j, cs = J & 3;
+                if (!mbar_wait_warp(&c_full[cs], (J >> 2) & 1, a.err)) { ok = false; break; }
+                tc_fence_after();
+#pragma unroll
+                for (int h = 0; h < T2_N / 16; h++) {
+                    if (g * T2_N + 16 * h >= P * P) break;
+                    float G[16];
+                    tmem_ld16(tl + (uint32_t)(cs * T2_N + 16 * h), G);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) {
+                        const int n = g * T2_N + 16 * h + i;
+                        if (n < P * P) acc[n % P] = fmaf(f1[n / P], G[i], acc[n % P]);
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&c_empty[cs]);
+            }
+            if (!ok) break;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
+            if (valid) {
+#pragma unroll
+                for (int p = 0; p < P; p++) {  // two-sum of the block total into (sum, correction)
+                    const float t = S[p] + acc[p], bpv = t - S[p];
+                    Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
+                    S[p] = t;
+                }
+            }
+            q++;
+        }
+        if (ok) {
+            const int D = D0 + d, vdf = (bt0 + j) * VB + v;
+            if (D < a.Nc && vdf < a.nvdf) {
+                const double sc = a.inv_scale[vdf];
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    double *dst = a.qacc + ((size_t)D * P + p) * a.NV + vdf;
+                    *dst += ((double)S[p] + (double)Cc[p]) * sc;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+static int tc2_prepare(Ctx *c)
+{
+    Layout &L = c->lay;
+    if (L.tc2_W) return DGV_OK;
+    const Grid &g = c->grid;
+    const int NG = t2_groups(g.P);
+    int rc = tc_value_scale(c, &L.tc2_vscale);
+    if (rc) return rc;
+    const size_t rec = (size_t)NG * T2_GREC;
+    cudaError_t e = cudaMalloc(&L.tc2_W, (size_t)std::max<long long>(1, L.nblocks) * rec);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        L.tc2_W = nullptr;
+        return set_err(c, DGV_ENOMEM, "tensor-core block form: no room for the block records");
+    }
+    if (L.nblocks)
+        k_tc2_build<<<(unsigned)L.nblocks, 256, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.P, g.Nc,
+                                                                 g.ccell, (float)L.tc2_vscale,
+                                                                 (unsigned char *)L.tc2_W);
+    DGV_CUDA(c, cudaGetLastError());
+    // block sets of about 48 MB of records: one launch each
+    L.tc2_sets.clear();
+    L.tc2_sets.push_back(0);
+    const long long per_set = std::max<long long>(1, (48LL << 20) / (long long)rec);
+    for (long long b = per_set; b < L.nblocks; b += per_set) L.tc2_sets.push_back((int)b);
+    if (L.tc2_sets.back() != (int)L.nblocks) L.tc2_sets.push_back((int)L.nblocks);
+    return DGV_OK;
+}
+
+template <int VB, int P>
+static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng)
+{
+    const size_t smem = (size_t)T2_NSTW * T2_GREC + 4 * (size_t)a.region + (2 * T2_NSTW + 13) * sizeof(uint64_t) + 16;
+    DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc2<VB, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    const Layout &L = c->lay;
+    KTimer kt(c);
+    for (size_t s = 0; s + 1 < L.tc2_sets.size(); s++) {
+        a.item_start = tl.item_start + s * (ng + 1);
+        a.tile_of = tl.tile_of + s * ng;
+        k_collide_tc2<VB, P><<<(unsigned)(a.nbp * ng), T2_THREADS, smem, c->stream>>>(a);
+        DGV_CUDA(c, cudaGetLastError());
+    }
+    kt.stop((long long)L.tc2_sets.size() - 1);
+    count_launches(c, (long long)L.tc2_sets.size() - 1);
+    return DGV_OK;
+}
+
+template <int P>
+static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, int VB)
+{
+    switch (VB) {
+    case 128: return launch_tc2<128, P>(c, a, tl, ng);
+    case 64: return launch_tc2<64, P>(c, a, tl, ng);
+    default: return launch_tc2<32, P>(c, a, tl, ng);
+    }
+}
+
+static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
+{
+    const Grid &g = c->grid;
+    Layout &L = c->lay;
+    int rc = tc2_prepare(c);
+    if (rc) return rc;
+    rc = ensure_errflag(c);
+    if (rc) return rc;
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), NDG = TC_ROWS / VB;
+    const int nbt = (nvdf + VB - 1) / VB, NV = nbt * VB, ng = (g.Nc + NDG - 1) / NDG;
+    const size_t fbytes = (size_t)nbt * g.Nc * g.P * VB * sizeof(float);
+    const size_t f16bytes = (size_t)nbt * 2 * g.Nc * VB * T2_K * 2;
+    const size_t qbytes = (size_t)g.N * NV * sizeof(double);
+    rc = ensure_buffer(c, &c->d_tcF, &c->tcF_bytes, fbytes + f16bytes + NV * sizeof(double));
+    if (rc) return rc;
+    rc = ensure_buffer(c, &c->d_tcQ, &c->tcQ_bytes, qbytes);
+    if (rc) return rc;
+    TcLists tl;
+    {
+        std::vector<int> first(L.nblocks), count(L.nblocks, 1);
+        std::iota(first.begin(), first.end(), 0);
+        rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl);
+        if (rc) return rc;
+    }
+    float *F = reinterpret_cast<float *>(c->d_tcF);
+    unsigned char *F16 = reinterpret_cast<unsigned char *>(c->d_tcF) + fbytes;
+    double *inv = reinterpret_cast<double *>(F16 + f16bytes);
+    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc2_vscale, F, inv, g.Nc, g.P, VB);
+    DGV_CUDA(c, cudaGetLastError());
+    k_tc2_f16<<<1184, 256, 0, c->stream>>>(F, F16, nbt, g.Nc, g.P, VB);
+    DGV_CUDA(c, cudaGetLastError());
+    DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
+    Tc2Args a;
+    a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.items = tl.items;
+    a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
+    a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt; a.nbp = (nbt + 1) / 2;
+    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + 1023) / 1024 * 1024;
+    rc = g.P == 27 ? launch_tc2_vb<27>(c, a, tl, ng, VB) : launch_tc2_vb<8>(c, a, tl, ng, VB);
+    if (rc) return rc;
+    long long tot = (long long)nvdf * g.N;
+    k_tc_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, c->d_nwt, d_q, g.N, nvdf, NV, scale);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 3);  // k_tc_fprep, k_tc2_f16, k_tc_final
+    if (c->project) return project_device(c, d_q, nvdf);
     return DGV_OK;
 }
 
@@ -721,6 +1168,7 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
     if (!L.blk) return set_err(c, DGV_ESTATE, "collide: no A-arrays loaded");
     if (g.P > 32) return set_err(c, DGV_EUNSUP, "tensor-core path: at most 32 nodes per cell");
     if (nvdf < 1) return set_err(c, DGV_EINVAL, "collide: batch must hold at least one VDF");
+    if (c->tc_form == 2 && (g.P == 27 || g.P == 8)) return collide_tc2_device(c, d_f, d_q, nvdf, scale);
     int rc = tc_prepare(c);
     if (rc) return rc;
     rc = ensure_errflag(c);

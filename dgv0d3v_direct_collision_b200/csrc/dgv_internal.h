@@ -71,7 +71,13 @@ struct Layout {
     double tc_vscale = 1.0;
     std::vector<int> tc_chunk_host;
     std::vector<int> tc_sets;
-    // device work lists {items, item starts, tile order}, keyed by cells per tile
+    // block form (built on first use): per block the dense split-fp16 tiles
+    // W[l2][(l1, p)] of its values, the value scale, and the block sets
+    void *tc2_W = nullptr;  // device
+    double tc2_vscale = 1.0;
+    std::vector<int> tc2_sets;
+    // device work lists {items, item starts, tile order}, keyed by cells per
+    // tile (chunk form) or 256 + cells per tile (block form)
     std::map<int, std::vector<void *>> tc_lists;
 };
 void free_layout(Layout &L);
@@ -122,6 +128,7 @@ struct Ctx {
     // kernel timing (DGV_OPT_KTIMING): event pairs around the collision
     // kernel's launches, summed on request; launch counters
     bool ktiming = false;
+    int tc_form = 1;  // DGV_OPT_TCFORM: 1 chunk form, 2 block form
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
     long long kt_launches = 0, kt_all = 0;
     double kt_ms = 0.0;

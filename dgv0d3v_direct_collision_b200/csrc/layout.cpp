@@ -28,6 +28,7 @@ void free_layout(Layout &L)
     for (auto &kv : L.chunks) cudaFree(kv.second);
     if (L.tc_V) cudaFree(L.tc_V);
     if (L.tc_chunk_start) cudaFree(L.tc_chunk_start);
+    if (L.tc2_W) cudaFree(L.tc2_W);
     for (auto &kv : L.tc_lists)
         for (void *p : kv.second) cudaFree(p);
     L = Layout();

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC, DGV_OPT_PROJECT,
-                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING)
+                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM)
 
 PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C, "tc": DGV_PREC_TC}
 
@@ -136,6 +136,11 @@ class DGVSolver:
 
     def set_nchunks(self, n: int):
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_NCHUNKS, int(n)))
+
+    def set_tc_form(self, form: int):
+        """Tensor-core form: 1 = pair chunks, 2 = dense cell-pair blocks
+        (grids of 8 or 27 nodes per cell; others keep the chunk form)."""
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCFORM, int(form)))
 
     def set_kernel_timing(self, on: bool):
         """Time the collision kernel's launches with CUDA events on the

@@ -1,0 +1,88 @@
+"""Parity of the block form of the tensor-core path (DGV_OPT_TCFORM = 2:
+G = f(c2) W on the tensor core, contraction with f(c1) on the CUDA cores)
+with the oracle, the golden vectors, the FP64 device path and the chunk form.
+Tolerance: 1e-6 norm-wise relative error, as for the chunk form."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from helpers import mixture_vdf
+
+pytestmark = pytest.mark.gpu
+
+TOLTC = 1e-6
+
+
+@pytest.fixture(scope="module")
+def c1():
+    """The 15^3 grid (s=3, M=5, [-6,6]^3) with seeded synthetic A on both sides."""
+    import dgv0d3v_direct_collision_b200 as m
+    from oracle.oracle import Oracle
+    o = Oracle(3, 5, 6.0)
+    o.set_A(*o.synth_A(seed=11, support=1))
+    s = m.DGVSolver(3, 5, 6.0)
+    s.generate_synthetic_A(seed=11, support=1)
+    s.set_tc_form(2)
+    return {"oracle": o, "solver": s}
+
+
+def test_tc2_golden(golden):
+    import dgv0d3v_direct_collision_b200 as m
+    s = m.DGVSolver(int(golden["s"]), int(golden["M"]), float(golden["L"]), kappa=float(golden["kappa"]))
+    s.load_A(golden["capphi"], golden["A"], golden["A_xi"], golden["A_xi1"], one_based=True)
+    s.set_tc_form(2)  # s = 2: 8 nodes per cell, one column group
+    q = s.EvalCollisionPeriodicAPlus_DGV(golden["f0"], precision="tc")
+    assert rel_err(q, golden["q0"]) < TOLTC
+
+
+def test_tc2_15cubed_vs_oracle(c1):
+    o, s = c1["oracle"], c1["solver"]
+    f = o.maxwellian(1.0, 1.5, 0, 0, 0.5) + o.maxwellian(1.0, -1.5, 0, 0, 0.5)
+    q = s.EvalCollisionPeriodicAPlus_DGV(f, precision="tc")
+    assert rel_err(q, o.collide(f)) < TOLTC
+
+
+@pytest.mark.parametrize("nb", [37, 150, 300])
+def test_tc2_batched_ragged(c1, nb):
+    """37: tiles of 64 VDFs x 2 cells, one tile; 150: two tiles of 128 (one
+    pair); 300: three tiles (the second CTA of a row tile has one); densities
+    over four decades; against the FP64 device path and the chunk form."""
+    o, s = c1["oracle"], c1["solver"]
+    rng = np.random.default_rng(5)
+    fs = np.stack([mixture_vdf(o.u, o.v, o.w, rng, normalise_w=o.gwts) * 10.0 ** rng.uniform(-2, 2)
+                   for _ in range(nb)])
+    q64 = s.EvalCollisionPeriodicAPlus_DGV(fs)
+    q2 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    s.set_tc_form(1)
+    try:
+        q1 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    finally:
+        s.set_tc_form(2)
+    for k in range(nb):
+        assert rel_err(q2[k], q64[k]) < TOLTC, k
+        assert rel_err(q2[k], q1[k]) < 2 * TOLTC, k
+    # one VDF alone (tiles of 32 VDFs x 4 cells)
+    assert rel_err(s.EvalCollisionPeriodicAPlus_DGV(fs[3], precision="tc"), q64[3]) < TOLTC
+
+
+def test_tc2_projection_and_rk_step(c1):
+    o, s = c1["oracle"], c1["solver"]
+    rng = np.random.default_rng(9)
+    f = mixture_vdf(o.u, o.v, o.w, rng, normalise_w=o.gwts)
+    q = s.EvalCollisionPeriodicAPlus_DGV(f)
+    s.set_projection(True)
+    try:
+        qp = s.EvalCollisionPeriodicAPlus_DGV(f, precision="tc")
+    finally:
+        s.set_projection(False)
+    for p in [np.ones(o.N), o.u, o.v, o.w, o.u ** 2 + o.v ** 2 + o.w ** 2]:
+        assert abs(np.sum(o.gwts * p * qp)) <= 1e-12 * np.sum(np.abs(o.gwts * p * q))
+    assert rel_err(qp, o.project(q)) < TOLTC
+    # RK2 steps through the captured graph (eager, capture, replay)
+    import torch
+    g = torch.from_numpy(f.copy()).cuda()
+    ref = f.copy()
+    for _ in range(3):
+        ref, _ = o.rk_step(ref, 0.01, 2)
+        s.TimeIntegratorORK_SH_DGV(g, 0.01, order=2, precision="tc")
+        assert rel_err(g.cpu().numpy() - f, ref - f) < TOLTC
