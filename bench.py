@@ -468,14 +468,17 @@ def run_profile_case(case: str):
     """Cases for profiler captures.  "<prec>_21": the 21^3 grid (s=3, M=7,
     [-6,6]^3; A rows ~5.6 GB in total) -- one VDF with a fixed chunk count (no
     tuning launches) for the CUDA-core kernels, a batch of 256 VDFs for the
-    tensor-core kernel (one launch per block set).  "tc_27": the benchmark
-    workload itself (27^3 x 256 VDFs), for single-pass counters only.  Two
-    evaluations each: a warm-up, then the one to capture."""
+    tensor-core kernels (one launch per block set; "tc" the chunk form, "tc2"
+    the block form).  "<prec>_15": the 15^3 grid (s=3, M=5, [-6,6]^3; rows
+    ~0.6 GB), 256 VDFs.  "<prec>_27": the benchmark workload itself (27^3 x
+    256 VDFs), for single-pass counters only.  Two evaluations each: a
+    warm-up, then the one to capture."""
     import torch
 
     import dgv0d3v_direct_collision_b200 as dgv
     prec, grid = case.split("_")
-    s = dgv.DGVSolver(S, M, L) if grid == "27" else dgv.DGVSolver(3, 7, 6.0)
+    s = {"27": lambda: dgv.DGVSolver(S, M, L), "21": lambda: dgv.DGVSolver(3, 7, 6.0),
+         "15": lambda: dgv.DGVSolver(3, 5, 6.0)}[grid]()
     s.generate_synthetic_A(seed=SEED_A, support=1)
     if prec == "tc2":
         s.set_tc_form(2)
@@ -500,7 +503,8 @@ def run_profile_case(case: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21", "tc_27", "tc2_21", "tc2_27"],
+    ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21", "tc_27", "tc2_21", "tc2_27",
+                                               "tc_15", "tc2_15"],
                     default=None,
                     help="small single-VDF case for profiler captures (no JSON bench line)")
     ap.add_argument("--gpus", type=int, default=1)

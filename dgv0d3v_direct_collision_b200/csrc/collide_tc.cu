@@ -111,6 +111,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// tcgen05.ld without its wait: the registers are valid after tmem_wait_ld()
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float *v)
 {
     uint32_t r[16];
@@ -990,15 +1003,21 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                 const int J = (q * NG + g) * nb2 + j, cs = J & 3;
                 if (!mbar_wait_warp(&c_full[cs], (J >> 2) & 1, a.err)) { ok = false; break; }
                 tc_fence_after();
+                // four 16-column loads in flight per wait: the load latency
+                // is paid twice per group instead of eight times
 #pragma unroll
-                for (int h = 0; h < T2_N / 16; h++) {
-                    if (g * T2_N + 16 * h >= P * P) break;
-                    float G[16];
-                    tmem_ld16(tl + (uint32_t)(cs * T2_N + 16 * h), G);
+                for (int hh = 0; hh < T2_N / 64; hh++) {
+                    if (g * T2_N + 64 * hh >= P * P) break;
+                    uint32_t G[64];
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        const int n = g * T2_N + 16 * h + i;
-                        if (n < P * P) acc[n % P] = fmaf(f1[n / P], G[i], acc[n % P]);
+                    for (int h = 0; h < 4; h++)
+                        if (g * T2_N + 64 * hh + 16 * h < P * P)
+                            tmem_ld16_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh + 16 * h), G + 16 * h);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 64; i++) {
+                        const int n = g * T2_N + 64 * hh + i;
+                        if (n < P * P) acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
                     }
                 }
                 tc_fence_before();
