@@ -973,35 +973,51 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             // FP32 accumulator, fp16 A (tensor memory) and B (shared memory,
             // K-major), M = 128, N = 128
             const uint32_t idesc = (1u << 4) | ((uint32_t)(T2_N >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            // The jobs (group g, VDF tile j) of a block are issued in pairs
+            // with their MMAs interleaved: consecutive instructions go to two
+            // different accumulators, so one does not wait for the other's
+            // accumulation to finish.
+            const int njob = NG * nb2;
             int q = 0, gw = 0, J = 0;
             bool ok = true;
             for (int it = i0; it < i1 && ok; it++) {
                 const int s = q & 1;
                 if (!mbar_wait(&a_ready[s], (q >> 1) & 1, a.err)) { ok = false; break; }
                 tc_fence_after();
-                for (int g = 0; g < NG && ok; g++, gw++) {
-                    const int st = gw % T2_NSTW;
-                    if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err)) { ok = false; break; }
-                    const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
-                    const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
-                    for (int j = 0; j < nb2; j++, J++) {
-                        const int cs = J % 3;
-                        if (!mbar_wait(&c_empty[cs], ((J / 3) & 1) ^ 1, a.err)) { ok = false; break; }
-                        tc_fence_after();
-                        // A of this item and VDF tile: hi in 16 columns, lo in the next 16
-                        const uint32_t ta = tmem + ACOL + (uint32_t)((2 * s + j) * 32);
-                        const uint32_t dacc = tmem + (uint32_t)(cs * T2_N);
-#pragma unroll
-                        for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 8 columns of A, 256 B of B
-                            umma_f16_ts(dacc, ta + 8 * t, dWh + 16 * t, idesc, t ? 1u : 0u);
-                            umma_f16_ts(dacc, ta + 8 * t, dWl + 16 * t, idesc, 1u);
-                            umma_f16_ts(dacc, ta + 16 + 8 * t, dWh + 16 * t, idesc, 1u);
-                        }
-                        umma_commit(&c_full[cs]);
+                for (int k = 0; k < njob && ok; k += 2) {
+                    const int nk = min(2, njob - k);
+                    uint64_t dWh[2], dWl[2];
+                    uint32_t ta[2], dacc[2];
+                    int cs[2];
+                    for (int u = 0; u < nk && ok; u++) {
+                        const int kk = k + u, g = kk / nb2, j = kk - g * nb2;
+                        const int gg = gw + g, st = gg % T2_NSTW;
+                        if (j == 0 && !mbar_wait(&w_full[st], (gg / T2_NSTW) & 1, a.err)) { ok = false; break; }
+                        cs[u] = (J + u) % 3;
+                        if (!mbar_wait(&c_empty[cs[u]], (((J + u) / 3) & 1) ^ 1, a.err)) { ok = false; break; }
+                        dWh[u] = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
+                        dWl[u] = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
+                        // A of this block and VDF tile: hi in 16 columns, lo in the next 16
+                        ta[u] = tmem + ACOL + (uint32_t)((2 * s + j) * 32);
+                        dacc[u] = tmem + (uint32_t)(cs[u] * T2_N);
                     }
                     if (!ok) break;
-                    umma_commit(&w_empty[st]);
+                    tc_fence_after();
+#pragma unroll
+                    for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 8 columns of A, 256 B of B
+                        for (int u = 0; u < nk; u++)
+                            umma_f16_ts(dacc[u], ta[u] + 8 * t, dWh[u] + 16 * t, idesc, t ? 1u : 0u);
+                        for (int u = 0; u < nk; u++) umma_f16_ts(dacc[u], ta[u] + 8 * t, dWl[u] + 16 * t, idesc, 1u);
+                        for (int u = 0; u < nk; u++) umma_f16_ts(dacc[u], ta[u] + 16 + 8 * t, dWh[u] + 16 * t, idesc, 1u);
+                    }
+                    for (int u = 0; u < nk; u++) {
+                        umma_commit(&c_full[cs[u]]);
+                        const int kk = k + u, g = kk / nb2, j = kk - g * nb2;
+                        if (j == nb2 - 1) umma_commit(&w_empty[(gw + g) % T2_NSTW]);  // last job of group g
+                    }
+                    J += nk;
                 }
+                gw += NG;
                 q++;
             }
             // every MMA issued so far completes before tensor memory is freed
