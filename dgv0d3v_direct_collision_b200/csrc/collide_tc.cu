@@ -738,7 +738,7 @@ static int tc_lists(Ctx *c, int NDG, TcLists *out)
 //   Q[(D,b), p] += sum_l1 f_b(c1+D, l1) * G[(D,b), (l1, p)],   G = F2 W,
 //   F2[(D,b), l2] = f_b(c2+D, l2).
 // G is a tensor-core product per block: M = 128 rows, K = 32 nodes l2
-// (zero-padded), N = P*P columns (l1, p) in groups of 128; F2 and W are split
+// (zero-padded), N = P*P columns (l1, p) in groups of 256; F2 and W are split
 // into fp16 hi + lo and hi*hi, hi*lo and lo*hi go into one FP32 accumulator.
 // The CUDA cores then contract each group of G with f(c1+D) in FP32 and add the
 // block total into a (sum, correction) pair with two-sum, in registers.  The
@@ -752,20 +752,17 @@ static int tc_lists(Ctx *c, int NDG, TcLists *out)
 //   warp 0     producer: TMA bulk copies of f (both tiles) and W groups
 //   warp 1     allocates all 512 tensor-memory columns; lane 0 issues MMAs
 //   warps 2-9  epilogue: warp w serves VDF tile (w-2)/4, tensor-memory lanes
-//              32*(w%4) .. +31 (one row per thread); it also copies its rows
-//              of the next block's A operand (f(c2+D) hi and lo) from shared
-//              into tensor memory
-// The A operand is read by the MMAs from tensor memory and only W from shared
-// memory: with both in shared memory an N = 128 MMA took ~133 cycles (shared
-// memory bandwidth), twice its arithmetic time.
-// Tensor memory: three accumulators of 128 columns used round-robin by the
-// (group, VDF tile) jobs (columns 0-383), and A for 2 blocks x 2 VDF tiles x
-// {hi, lo} x 16 columns (384-511).  Every wait is bounded, as in the chunk form.
-constexpr int T2_N = 128;                     // columns (l1, p) per group
+//              32*(w%4) .. +31 (one row per thread)
+// Tensor memory: two accumulators of 256 columns, used alternately by the
+// (group, VDF tile) jobs.  Measured on B200: an M = 128 MMA costs ~130 cycles
+// at N = 128 whether A comes from shared or tensor memory, and about the same
+// at N = 256, so the wide groups halve the MMA time of a block.  Every wait is
+// bounded, as in the chunk form.
+constexpr int T2_N = 256;                     // columns (l1, p) per group
 constexpr int T2_K = 32;                      // nodes l2 per block, zero-padded
-constexpr int T2_TILE = T2_N * T2_K * 2;      // one fp16 tile (8 KiB)
+constexpr int T2_TILE = T2_N * T2_K * 2;      // one fp16 tile (16 KiB)
 constexpr int T2_GREC = 2 * T2_TILE;          // hi and lo tiles of one group
-constexpr int T2_NSTW = 4;                    // W ring stages
+constexpr int T2_NSTW = 3;                    // W ring stages
 constexpr int T2_ATILE = TC_ROWS * T2_K * 2;  // 128 rows x 32 fp16 (8 KiB)
 constexpr int T2_EPI_WARPS = 8;
 constexpr int T2_THREADS = 32 * (2 + T2_EPI_WARPS);
@@ -807,16 +804,9 @@ __global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64
     }
 }
 
-// F16[((bt*2 + h)*Nc + cell) * VB*64 + t2_foff(v, l, VB)]: per VDF tile and
-// cell VB rows (VDFs) x 32 nodes, h = 0 hi / 1 lo parts of the scaled FP32
-// copy F[((bt*Nc + cell)*P + l)*VB + v]; nodes l >= P are zero.  Within a
-// cell the 16-byte chunks (8 nodes) of all rows are grouped by chunk, so the
-// 32 lanes of a warp (32 consecutive rows) read 512 contiguous bytes
-__host__ __device__ __forceinline__ int t2_foff(int v, int l, int VB)
-{
-    return (l >> 3) * VB * 16 + v * 16 + (l & 7) * 2;
-}
-
+// F16[((bt*2 + h)*Nc + cell) * VB*64 + t2_off(v, l)]: per VDF tile and cell a
+// tile of VB rows (VDFs) x 32 nodes, h = 0 hi / 1 lo parts of the scaled FP32
+// copy F[((bt*Nc + cell)*P + l)*VB + v]; nodes l >= P are zero
 __global__ void k_tc2_f16(const float *F, unsigned char *F16, int nbt, int Nc, int P, int VB)
 {
     const long long total = (long long)nbt * Nc * T2_K * VB;
@@ -831,7 +821,7 @@ __global__ void k_tc2_f16(const float *F, unsigned char *F16, int nbt, int Nc, i
         const float x = l < P ? F[(((size_t)bt * Nc + cell) * P + l) * VB + v] : 0.f;
         const __half h = __float2half_rn(x);
         const __half lo = __float2half_rn(x - __half2float(h));
-        unsigned char *base = F16 + ((size_t)(2 * bt) * Nc + cell) * tile + t2_foff(v, l, VB);
+        unsigned char *base = F16 + ((size_t)(2 * bt) * Nc + cell) * tile + t2_off(v, l);
         *reinterpret_cast<__half *>(base) = h;
         *reinterpret_cast<__half *>(base + (size_t)Nc * tile) = lo;
     }
@@ -851,36 +841,19 @@ struct Tc2Args {
     int region;  // bytes per VDF tile in an item slot: A hi, A lo, f(c1) (FP32)
 };
 
-// non-blocking test of a phase (no suspension), same outcome for the warp
-__device__ __forceinline__ bool mbar_test_warp(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return __all_sync(0xffffffffu, ok != 0);
-}
-
 template <int VB, int P>
 __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
 {
     constexpr int NDG = TC_ROWS / VB;
     constexpr int NG = t2_groups(P);
-    constexpr int G_STAGE = NG > 1 ? 1 : 0;  // group after which the next item's A is staged, at the earliest
-    constexpr uint32_t ACOL = 3 * T2_N;      // tensor-memory columns of the A operands
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *wring = smem;                      // T2_NSTW x T2_GREC
     unsigned char *slots = smem + T2_NSTW * T2_GREC;  // 2 item slots x 2 VDF tiles x region
     uint64_t *bars = reinterpret_cast<uint64_t *>(slots + 4 * a.region);
     uint64_t *w_full = bars, *w_empty = bars + T2_NSTW;
     uint64_t *s_full = w_empty + T2_NSTW, *s_empty = s_full + 2;
-    uint64_t *a_ready = s_empty + 2;
-    uint64_t *c_full = a_ready + 2, *c_empty = c_full + 3;
-    uint64_t *drain = c_empty + 3;
+    uint64_t *c_full = s_empty + 2, *c_empty = c_full + 2;
+    uint64_t *drain = c_empty + 4;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -895,10 +868,9 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         }
         for (int s = 0; s < 2; s++) {
             mbar_init(&s_full[s], 1);
-            mbar_init(&s_empty[s], 4 * nb2);  // epilogue warps: f(c1) read, A staged
-            mbar_init(&a_ready[s], 4 * nb2);  // epilogue warps: A written to tensor memory
+            mbar_init(&s_empty[s], 1 + 4 * nb2);  // the MMA commit + the epilogue warps
         }
-        for (int s = 0; s < 3; s++) {
+        for (int s = 0; s < 2; s++) {
             mbar_init(&c_full[s], 1);
             mbar_init(&c_empty[s], 4);
         }
@@ -926,7 +898,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                 const int s = q & 1;
                 if (!mbar_wait(&s_empty[s], ((q >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
                 // f of cells c1 + D - ccell (FP32) and c2 + D - ccell (fp16
-                // hi and lo), D in the row tile, clipped to the grid
+                // tiles), D in the row tile, clipped to the grid
                 const int cs1 = e.c1 + D0 - a.ccell, cs2 = e.c2 + D0 - a.ccell;
                 const int lo1 = max(cs1, 0), hi1 = min(cs1 + NDG, a.Nc);
                 const int lo2 = max(cs2, 0), hi2 = min(cs2 + NDG, a.Nc);
@@ -970,54 +942,39 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            // FP32 accumulator, fp16 A (tensor memory) and B (shared memory,
-            // K-major), M = 128, N = 128
+            // FP32 accumulator, fp16 A and B, both K-major, M = 128, N = 128
             const uint32_t idesc = (1u << 4) | ((uint32_t)(T2_N >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
-            // The jobs (group g, VDF tile j) of a block are issued in pairs
-            // with their MMAs interleaved: consecutive instructions go to two
-            // different accumulators, so one does not wait for the other's
-            // accumulation to finish.
-            const int njob = NG * nb2;
             int q = 0, gw = 0, J = 0;
             bool ok = true;
             for (int it = i0; it < i1 && ok; it++) {
                 const int s = q & 1;
-                if (!mbar_wait(&a_ready[s], (q >> 1) & 1, a.err)) { ok = false; break; }
-                tc_fence_after();
-                for (int k = 0; k < njob && ok; k += 2) {
-                    const int nk = min(2, njob - k);
-                    uint64_t dWh[2], dWl[2];
-                    uint32_t ta[2], dacc[2];
-                    int cs[2];
-                    for (int u = 0; u < nk && ok; u++) {
-                        const int kk = k + u, g = kk / nb2, j = kk - g * nb2;
-                        const int gg = gw + g, st = gg % T2_NSTW;
-                        if (j == 0 && !mbar_wait(&w_full[st], (gg / T2_NSTW) & 1, a.err)) { ok = false; break; }
-                        cs[u] = (J + u) % 3;
-                        if (!mbar_wait(&c_empty[cs[u]], (((J + u) / 3) & 1) ^ 1, a.err)) { ok = false; break; }
-                        dWh[u] = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
-                        dWl[u] = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
-                        // A of this block and VDF tile: hi in 16 columns, lo in the next 16
-                        ta[u] = tmem + ACOL + (uint32_t)((2 * s + j) * 32);
-                        dacc[u] = tmem + (uint32_t)(cs[u] * T2_N);
+                if (!mbar_wait(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
+                for (int g = 0; g < NG && ok; g++, gw++) {
+                    const int st = gw % T2_NSTW;
+                    if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err)) { ok = false; break; }
+                    const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
+                    const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
+                    for (int j = 0; j < nb2; j++, J++) {
+                        const int cs = J & 1;
+                        if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
+                        tc_fence_after();
+                        unsigned char *reg = slots + (size_t)(2 * s + j) * a.region;
+                        const uint64_t dAh = umma_desc(smem_u32(reg), 128, 512);
+                        const uint64_t dAl = umma_desc(smem_u32(reg + T2_ATILE), 128, 512);
+                        const uint32_t dacc = tmem + (uint32_t)(cs * T2_N);
+#pragma unroll
+                        for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 256 B along K
+                            umma_f16(dacc, dAh + 16 * t, dWh + 16 * t, idesc, t ? 1u : 0u);
+                            umma_f16(dacc, dAh + 16 * t, dWl + 16 * t, idesc, 1u);
+                            umma_f16(dacc, dAl + 16 * t, dWh + 16 * t, idesc, 1u);
+                        }
+                        umma_commit(&c_full[cs]);
                     }
                     if (!ok) break;
-                    tc_fence_after();
-#pragma unroll
-                    for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 8 columns of A, 256 B of B
-                        for (int u = 0; u < nk; u++)
-                            umma_f16_ts(dacc[u], ta[u] + 8 * t, dWh[u] + 16 * t, idesc, t ? 1u : 0u);
-                        for (int u = 0; u < nk; u++) umma_f16_ts(dacc[u], ta[u] + 8 * t, dWl[u] + 16 * t, idesc, 1u);
-                        for (int u = 0; u < nk; u++) umma_f16_ts(dacc[u], ta[u] + 16 + 8 * t, dWh[u] + 16 * t, idesc, 1u);
-                    }
-                    for (int u = 0; u < nk; u++) {
-                        umma_commit(&c_full[cs[u]]);
-                        const int kk = k + u, g = kk / nb2, j = kk - g * nb2;
-                        if (j == nb2 - 1) umma_commit(&w_empty[(gw + g) % T2_NSTW]);  // last job of group g
-                    }
-                    J += nk;
+                    umma_commit(&w_empty[st]);
                 }
-                gw += NG;
+                if (!ok) break;
+                umma_commit(&s_empty[s]);
                 q++;
             }
             // every MMA issued so far completes before tensor memory is freed
@@ -1030,36 +987,13 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         const int j = (warp - 2) / 4, quarter = warp & 3, r = quarter * 32 + lane;
         const uint32_t tl = tmem + ((uint32_t)(quarter * 32) << 16);
         const int d = r / VB, v = r % VB;
-        const int nit = i1 - i0;
-        // this row's A operand of item slot s: f(c2+D) hi and lo (32 nodes,
-        // 16 columns each) from shared into tensor memory
-        auto stage_a = [&](int s) {
-            const unsigned char *src = slots + (size_t)(2 * s + j) * a.region + (size_t)d * VB * 64 + (size_t)v * 16;
-            uint32_t hw[16], lw[16];
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const uint4 x = *reinterpret_cast<const uint4 *>(src + c * VB * 16);
-                const uint4 y = *reinterpret_cast<const uint4 *>(src + T2_ATILE + c * VB * 16);
-                hw[4 * c] = x.x; hw[4 * c + 1] = x.y; hw[4 * c + 2] = x.z; hw[4 * c + 3] = x.w;
-                lw[4 * c] = y.x; lw[4 * c + 1] = y.y; lw[4 * c + 2] = y.z; lw[4 * c + 3] = y.w;
-            }
-            tmem_st16u(tl + ACOL + (uint32_t)((2 * s + j) * 32), hw);
-            tmem_st16u(tl + ACOL + (uint32_t)((2 * s + j) * 32 + 16), lw);
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&a_ready[s]);
-        };
         float S[P], Cc[P];
 #pragma unroll
         for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
+        int q = 0;
         bool ok = true;
-        if (nit > 0) {
-            if (mbar_wait_warp(&s_full[0], 0, a.err)) stage_a(0);
-            else ok = false;
-        }
-        for (int q = 0; q < nit && ok; q++) {
-            const bool valid = (a.items[i0 + q].nch >> (16 + d)) & 1;
+        for (int it = i0; it < i1 && ok; it++) {
+            const bool valid = (a.items[it].nch >> (16 + d)) & 1;
             const int s = q & 1;
             if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
             const float *f1s =
@@ -1067,18 +1001,13 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             float f1[P], acc[P];
 #pragma unroll
             for (int l = 0; l < P; l++) { f1[l] = f1s[l * VB]; acc[l] = 0.f; }
-            // the next item's A is staged as soon as its f has landed (at the
-            // latest after the last group): its tensor-memory slot was last
-            // read by MMAs that completed before the accumulators waited on here
-            bool staged = q + 1 >= nit;
-            const int s1 = (q + 1) & 1;
-            const uint32_t par1 = ((q + 1) >> 1) & 1;
 #pragma unroll
             for (int g = 0; g < NG; g++) {
-                const int J = (q * NG + g) * nb2 + j, cs = J % 3;
-                if (!mbar_wait_warp(&c_full[cs], (J / 3) & 1, a.err)) { ok = false; break; }
+                const int J = (q * NG + g) * nb2 + j, cs = J & 1;
+                if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, a.err)) { ok = false; break; }
                 tc_fence_after();
-                // four 16-column loads in flight per wait
+                // four 16-column loads in flight per wait: the load latency
+                // is paid twice per group instead of eight times
 #pragma unroll
                 for (int hh = 0; hh < T2_N / 64; hh++) {
                     if (g * T2_N + 64 * hh >= P * P) break;
@@ -1097,16 +1026,6 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&c_empty[cs]);
-                if (!staged && g >= G_STAGE) {
-                    if (g == NG - 1) {
-                        if (!mbar_wait_warp(&s_full[s1], par1, a.err)) { ok = false; break; }
-                        stage_a(s1);
-                        staged = true;
-                    } else if (mbar_test_warp(&s_full[s1], par1)) {
-                        stage_a(s1);
-                        staged = true;
-                    }
-                }
             }
             if (!ok) break;
             __syncwarp();
@@ -1119,6 +1038,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                     S[p] = t;
                 }
             }
+            q++;
         }
         if (ok) {
             const int D = D0 + d, vdf = (bt0 + j) * VB + v;
