@@ -202,11 +202,13 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def load_profile_traffic():
+def load_profile_traffic(form: int):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/k_collide_tc_27cubed_b256.json), or None."""
+    summary (profiles/k_collide_tc2_27cubed_b256.json for the block form,
+    k_collide_tc_27cubed_b256.json for the chunk form), or None."""
+    name = "k_collide_tc2_27cubed_b256.json" if form == 2 else "k_collide_tc_27cubed_b256.json"
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "k_collide_tc_27cubed_b256.json")))
+        d = json.load(open(os.path.join(ROOT, "profiles", name)))
         return float(d["dram_bytes_per_launch"]), d.get("note", "")
     except Exception:
         return None, ""
@@ -315,7 +317,15 @@ def run_ours(args, world, rank, local):
     k_ms_launch = kst["ms"] / max(kst["launches"], 1)
     alg_flop_launch = alg_flop_eval * BATCH * args.steps / max(kst["launches"], 1)
     achieved = alg_flop_launch / (k_ms_launch / 1000.0) / 1e12
-    traffic, tnote = load_profile_traffic()
+    form = solver.tc_form
+    traffic, tnote = load_profile_traffic(form)
+    kname = "k_collide_tc2<128,27>" if form == 2 else "k_collide_tc<128>"
+    knote = ("algorithmic FLOPs = 3 per record-shift (A*f*f + add) x VDFs; the block form computes "
+             "G = f(c2) W per cell-pair block on the tensor core (dense W: 27 x 729 per block, 3 fp16 "
+             "products hi*hi, hi*lo, lo*hi, M=128 x N=256 tiles) and contracts G with f(c1) on the CUDA cores. "
+             if form == 2 else
+             "algorithmic FLOPs = 3 per record-shift (A*f*f + add) x VDFs; the kernel issues "
+             "3 fp16 products per term (hi*hi, hi*lo, lo*hi) on M=128 x N<=64 tiles. ")
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -324,22 +334,22 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD, "grid": "s=3,M=9,L=7", "batch_per_gpu": BATCH, "global_batch": BATCH * world,
                    "precision": "tensor cores (tcgen05): split-fp16 operands, compensated FP32/FP64 accumulation, "
                                 "FP64 conservation projection",
+                   "tc_form": "block (dense cell-pair W, DGV_OPT_TCFORM=2)" if form == 2 else "chunk (pairs, DGV_OPT_TCFORM=1)",
                    "A": f"seeded synthetic records, reference index structure: {info['records']} records, "
                         f"{info['pairs']} pairs, {info['blocks']} cell-pair blocks",
                    "record_shifts_per_eval": info["record_shifts"],
-                   "l2": "inputs larger than L2: A chunk records (~8 GB) are streamed from HBM every step",
+                   "l2": "inputs larger than L2: the A records (~14.6 GB block form / ~8 GB chunk form) "
+                         "are streamed from HBM every step",
                    "parallelism": f"replicas over VDFs, dp{world}"},
         "f64_plain_evals_per_s": value64, "f64_timed_vdfs": NB64, "tc_over_f64": value / value64,
         "err_tc_vs_f64_norm_max": float(errs.max()), "err_tc_vs_f64_maxabs_rel_max": float(merrs.max()),
         "conservation_rel_max": float(cons),
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
                      "frac": achieved / tc_peak, "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "k_collide_tc<128>", "launches_per_step": kst["launches"] / args.steps,
+                     "kernel": kname, "launches_per_step": kst["launches"] / args.steps,
                      "kernel_ms_per_launch": k_ms_launch,
                      "alg_flop_per_launch": alg_flop_launch,
-                     "note": "algorithmic FLOPs = 3 per record-shift (A*f*f + add) x VDFs; the kernel issues "
-                             "3 fp16 products per term (hi*hi, hi*lo, lo*hi) on M=128 x N<=64 tiles. "
-                             "traffic = ncu dram read+write bytes per launch. " + tnote},
+                     "note": knote + "traffic = ncu dram read+write bytes per launch. " + tnote},
         "cpu_baseline": None,
         "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(BATCH * N * 8),
                 "d2h_bytes_per_step": int(BATCH * N * 8)},

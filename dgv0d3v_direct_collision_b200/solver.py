@@ -83,6 +83,7 @@ class DGVSolver:
         self.device = device
         self.kappa = float(kappa)
         self.projection = False
+        self.tc_form = 2
 
     # -- plumbing ------------------------------------------------------------
     def _check(self, rc: int):
@@ -138,9 +139,10 @@ class DGVSolver:
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_NCHUNKS, int(n)))
 
     def set_tc_form(self, form: int):
-        """Tensor-core form: 1 = pair chunks, 2 = dense cell-pair blocks
-        (grids of 8 or 27 nodes per cell; others keep the chunk form)."""
+        """Tensor-core form: 2 (default) = dense cell-pair blocks (grids of 8
+        or 27 nodes per cell; others use the chunk form), 1 = pair chunks."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCFORM, int(form)))
+        self.tc_form = int(form)
 
     def set_kernel_timing(self, on: bool):
         """Time the collision kernel's launches with CUDA events on the

@@ -54,10 +54,11 @@ extern "C" {
 #define DGV_OPT_NCHUNKS 2  /* work chunks per VDF (0 = autotune)             */
 #define DGV_OPT_KTIMING 3  /* 1: time the collision kernel with CUDA events   */
                            /* on the context stream (read: dgv_kernel_stats)  */
-#define DGV_OPT_TCFORM 4   /* tensor-core form: 1 = pair chunks (products    */
-                           /* formed per pair), 2 = dense cell-pair blocks    */
-                           /* (f(c2) x W on the tensor core, then f(c1) on    */
-                           /* the CUDA cores; 8 or 27 nodes per cell)         */
+#define DGV_OPT_TCFORM 4   /* tensor-core form: 2 (default) = dense cell-pair */
+                           /* blocks (f(c2) x W on the tensor core, then      */
+                           /* f(c1) on the CUDA cores; grids of 8 or 27 nodes */
+                           /* per cell, others use form 1), 1 = pair chunks   */
+                           /* (products formed per pair on the CUDA cores)    */
 
 typedef struct dgv_ctx dgv_ctx;
 

@@ -1,6 +1,8 @@
-"""Parity of the tensor-core collision path (DGV_PREC_TC, tcgen05 with
+"""Parity of the chunk form of the tensor-core collision path (DGV_PREC_TC
+with DGV_OPT_TCFORM = 1: products per pair on the CUDA cores, tcgen05 with
 split-fp16 operands) with the oracle, the golden vectors and the FP64 device
-path.  Tolerance: 1e-6 norm-wise relative error, the bound the batched
+path.  The block form (the default) is covered in test_gpu_tc2.py.
+Tolerance: 1e-6 norm-wise relative error, the bound the batched
 reduced-precision path is held to."""
 import numpy as np
 import pytest
@@ -23,6 +25,7 @@ def dgv():
 def gsolver(dgv, golden):
     s = dgv.DGVSolver(int(golden["s"]), int(golden["M"]), float(golden["L"]), kappa=float(golden["kappa"]))
     s.load_A(golden["capphi"], golden["A"], golden["A_xi"], golden["A_xi1"], one_based=True)
+    s.set_tc_form(1)
     return s
 
 
@@ -36,6 +39,7 @@ def c1():
     o.set_A(cap, A, xi, xi1)
     s = m.DGVSolver(3, 5, 6.0)
     s.generate_synthetic_A(seed=11, support=1)
+    s.set_tc_form(1)
     return {"oracle": o, "solver": s}
 
 
