@@ -111,18 +111,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// tcgen05.ld without its wait: the registers are valid after tmem_wait_ld()
-__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t *r)
+// registers written by the tcgen05.ld forms below are valid after tmem_wait_ld()
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 32 consecutive columns of this warp's lane quarter in one instruction (no wait)
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t *r)
 {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]),"=r"(r[1]),"=r"(r[2]),"=r"(r[3]),"=r"(r[4]),"=r"(r[5]),"=r"(r[6]),"=r"(r[7]),"=r"(r[8]),"=r"(r[9]),"=r"(r[10]),"=r"(r[11]),"=r"(r[12]),"=r"(r[13]),"=r"(r[14]),"=r"(r[15]),"=r"(r[16]),"=r"(r[17]),"=r"(r[18]),"=r"(r[19]),"=r"(r[20]),"=r"(r[21]),"=r"(r[22]),"=r"(r[23]),"=r"(r[24]),"=r"(r[25]),"=r"(r[26]),"=r"(r[27]),"=r"(r[28]),"=r"(r[29]),"=r"(r[30]),"=r"(r[31])
+                 : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float *v)
 {
@@ -1006,16 +1005,14 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                 const int J = (q * NG + g) * nb2 + j, cs = J & 1;
                 if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, a.err)) { ok = false; break; }
                 tc_fence_after();
-                // four 16-column loads in flight per wait: the load latency
-                // is paid twice per group instead of eight times
+                // two 32-column loads per wait: the load latency is paid
+                // four times per 256-column group
 #pragma unroll
                 for (int hh = 0; hh < T2_N / 64; hh++) {
                     if (g * T2_N + 64 * hh >= P * P) break;
                     uint32_t G[64];
-#pragma unroll
-                    for (int h = 0; h < 4; h++)
-                        if (g * T2_N + 64 * hh + 16 * h < P * P)
-                            tmem_ld16_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh + 16 * h), G + 16 * h);
+                    tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh), G);
+                    if (g * T2_N + 64 * hh + 32 < P * P) tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh + 32), G + 32);
                     tmem_wait_ld();
 #pragma unroll
                     for (int i = 0; i < 64; i++) {
