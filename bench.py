@@ -224,6 +224,8 @@ def run_ours(args, world, rank, local):
     solver.set_stream(stream.cuda_stream)
     if args.tc_form:
         solver.set_tc_form(args.tc_form)
+    if args.tc_tiles:
+        solver.set_tc_tiles_per_cta(args.tc_tiles)
     t = time.perf_counter()
     solver.generate_synthetic_A(seed=SEED_A, support=1)
     t_gen = time.perf_counter() - t
@@ -532,6 +534,8 @@ def main():
     ap.add_argument("--trajectory-steps", type=int, default=500)
     ap.add_argument("--tc-form", type=int, default=0, choices=[0, 1, 2],
                     help="tensor-core form of the headline arm (0 = the library default)")
+    ap.add_argument("--tc-tiles", type=int, default=0, choices=[0, 1, 2],
+                    help="block form: VDF tiles per CTA (0 = the library default)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

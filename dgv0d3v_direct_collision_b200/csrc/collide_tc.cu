@@ -837,6 +837,7 @@ struct Tc2Args {
     const double *inv_scale;   // [NV]
     int *err;
     int Nc, ccell, NV, nvdf, nbt, nbp;
+    int tpc;     // VDF tiles per CTA (1 or 2)
     int region;  // bytes per VDF tile in an item slot: A hi, A lo, f(c1) (FP32)
 };
 
@@ -857,7 +858,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bp = blockIdx.x % a.nbp, ti = blockIdx.x / a.nbp;
-    const int bt0 = 2 * bp, nb2 = min(2, a.nbt - bt0);
+    const int bt0 = a.tpc * bp, nb2 = min(a.tpc, a.nbt - bt0);
     const int D0 = a.tile_of[ti] * NDG;
     const int i0 = a.item_start[ti], i1 = a.item_start[ti + 1];
     if (threadIdx.x == 0) {
@@ -1149,7 +1150,9 @@ static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, 
     Tc2Args a;
     a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.items = tl.items;
     a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
-    a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt; a.nbp = (nbt + 1) / 2;
+    a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
+    a.tpc = c->tc_tiles_per_cta;
+    a.nbp = (nbt + a.tpc - 1) / a.tpc;
     a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + 1023) / 1024 * 1024;
     rc = g.P == 27 ? launch_tc2_vb<27>(c, a, tl, ng, VB) : launch_tc2_vb<8>(c, a, tl, ng, VB);
     if (rc) return rc;

@@ -129,6 +129,7 @@ struct Ctx {
     // kernel's launches, summed on request; launch counters
     bool ktiming = false;
     int tc_form = 2;  // DGV_OPT_TCFORM: 1 chunk form, 2 block form (8 or 27 nodes per cell)
+    int tc_tiles_per_cta = 2;  // DGV_OPT_TCTILES: VDF tiles per CTA in the block form
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
     long long kt_launches = 0, kt_all = 0;
     double kt_ms = 0.0;

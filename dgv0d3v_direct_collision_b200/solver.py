@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC, DGV_OPT_PROJECT,
-                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM)
+                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM, DGV_OPT_TCTILES)
 
 PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C, "tc": DGV_PREC_TC}
 
@@ -143,6 +143,10 @@ class DGVSolver:
         or 27 nodes per cell; others use the chunk form), 1 = pair chunks."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCFORM, int(form)))
         self.tc_form = int(form)
+
+    def set_tc_tiles_per_cta(self, n: int):
+        """Block form: VDF tiles (of up to 128) per CTA, 2 or 1."""
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCTILES, int(n)))
 
     def set_kernel_timing(self, on: bool):
         """Time the collision kernel's launches with CUDA events on the

@@ -59,6 +59,9 @@ extern "C" {
                            /* f(c1) on the CUDA cores; grids of 8 or 27 nodes */
                            /* per cell, others use form 1), 1 = pair chunks   */
                            /* (products formed per pair on the CUDA cores)    */
+#define DGV_OPT_TCTILES 5  /* block form: VDF tiles of 128 per CTA, 2 (one W  */
+                           /* read from L2 per 256 rows, one accumulator per  */
+                           /* tile) or 1 (two accumulators per tile)          */
 
 typedef struct dgv_ctx dgv_ctx;
 

@@ -86,3 +86,21 @@ def test_tc2_projection_and_rk_step(c1):
         ref, _ = o.rk_step(ref, 0.01, 2)
         s.TimeIntegratorORK_SH_DGV(g, 0.01, order=2, precision="tc")
         assert rel_err(g.cpu().numpy() - f, ref - f) < TOLTC
+
+
+def test_tc2_one_tile_per_cta(c1):
+    """DGV_OPT_TCTILES = 1: each CTA serves one VDF tile with two alternating
+    accumulators; same results as two tiles per CTA."""
+    o, s = c1["oracle"], c1["solver"]
+    rng = np.random.default_rng(17)
+    fs = np.stack([mixture_vdf(o.u, o.v, o.w, rng, normalise_w=o.gwts) for _ in range(150)])
+    q2 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    s.set_tc_tiles_per_cta(1)
+    try:
+        q1 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    finally:
+        s.set_tc_tiles_per_cta(2)
+    q64 = s.EvalCollisionPeriodicAPlus_DGV(fs[:8])
+    for k in range(8):
+        assert rel_err(q1[k], q64[k]) < TOLTC, k
+    assert rel_err(q1, q2) < 1e-9  # same per-row arithmetic, only the CTA split differs
