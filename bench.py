@@ -244,6 +244,7 @@ def run_ours(args, world, rank, local):
         step()  # first call builds the tensor-core layout and work lists
         torch.cuda.synchronize()
     t_prep = time.perf_counter() - t
+    plan = solver.tc_plan(BATCH)  # the records and lists exist now
     solver.set_kernel_timing(True)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup - 1):
@@ -319,6 +320,8 @@ def run_ours(args, world, rank, local):
     k_ms_launch = kst["ms"] / max(kst["launches"], 1)
     alg_flop_launch = alg_flop_eval * BATCH * args.steps / max(kst["launches"], 1)
     achieved = alg_flop_launch / (k_ms_launch / 1000.0) / 1e12
+    # FLOPs the MMAs issue per launch (dense tiles, three split products) over the same time
+    issued = plan["tensor_flop"] / max(plan["launches"], 1) / (k_ms_launch / 1000.0) / 1e12
     form = solver.tc_form
     traffic, tnote = load_profile_traffic(form)
     kname = "k_collide_tc2<128,27>" if form == 2 else "k_collide_tc<128>"
@@ -349,6 +352,8 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
                      "frac": achieved / tc_peak, "traffic": traffic, "peak_source": peak_src,
                      "kernel": kname, "launches_per_step": kst["launches"] / args.steps,
+                     "issued_tensor_tflops": issued, "issued_frac": issued / tc_peak,
+                     "issued_over_algorithmic": plan["tensor_flop"] / (alg_flop_eval * BATCH),
                      "kernel_ms_per_launch": k_ms_launch,
                      "alg_flop_per_launch": alg_flop_launch,
                      "note": knote + "traffic = ncu dram read+write bytes per launch. " + tnote},

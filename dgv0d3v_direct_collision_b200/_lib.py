@@ -28,7 +28,7 @@ EXPORTS = [
     "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
     "dgv_compute_A", "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
     "dgv_write_solution", "dgv_read_solution", "dgv_write_solution_arrays", "dgv_read_solution_arrays",
-    "dgv_collide_group",
+    "dgv_collide_group", "dgv_tc_plan",
 ]
 
 
@@ -77,6 +77,7 @@ def load() -> C.CDLL:
         "dgv_collide_batched": [vp, i32, vp, vp, C.c_int],
         "dgv_collide_cells": [vp, i32, vp, vp, i32, i32, C.c_int],
         "dgv_collide_group": [i32, C.POINTER(vp), vp, vp, vp, C.c_int, vp],
+        "dgv_tc_plan": [vp, i32, C.POINTER(i64), C.POINTER(i64), C.POINTER(dbl)],
         "dgv_compute_A": [vp, dbl, dbl, dbl, dbl, C.c_int],
         "dgv_read_A_files": [vp, C.POINTER(C.c_char_p), i32],
         "dgv_write_A_file": [vp, C.c_char_p, i64],

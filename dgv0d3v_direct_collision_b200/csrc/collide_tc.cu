@@ -713,6 +713,9 @@ static int tc_work_lists(Ctx *c, int NDG, int key, const std::vector<int> &sets,
     DGV_CUDA(c, cudaMemcpy(d[1], start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
     DGV_CUDA(c, cudaMemcpy(d[2], tile_of.data(), sizeof(int) * tile_of.size(), cudaMemcpyHostToDevice));
     L.tc_lists[key] = {d[0], d[1], d[2]};
+    long long wsum = 0;
+    for (const TcItem &e : items) wsum += e.nch & 0xffff;
+    L.tc_list_work[key] = wsum;
     out->items = reinterpret_cast<TcItem *>(d[0]);
     out->item_start = reinterpret_cast<int *>(d[1]);
     out->tile_of = reinterpret_cast<int *>(d[2]);
@@ -1183,6 +1186,40 @@ static int launch_tc(Ctx *c, TcArgs &a, const TcLists &tl, int ng)
     return DGV_OK;
 }
 
+// Work plan of one tensor-core evaluation of nvdf VDFs in the current form:
+// kernel launches, work items (block x row tile, or chunk x row tile) summed
+// over the VDF tiles, and the FLOPs the MMAs issue (dense tiles, all three
+// split products).  Builds the records and lists if they do not exist yet.
+int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flop)
+{
+    const Grid &g = c->grid;
+    Layout &L = c->lay;
+    if (!L.blk) return set_err(c, DGV_ESTATE, "tc_plan: no A-arrays loaded");
+    if (g.P > 32 || nvdf < 1) return set_err(c, DGV_EINVAL, "tc_plan: no tensor-core plan for this grid or batch");
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), NDG = TC_ROWS / VB;
+    const long long nbt = (nvdf + VB - 1) / VB;
+    TcLists tl;
+    int rc;
+    if (c->tc_form == 2 && (g.P == 27 || g.P == 8)) {
+        if ((rc = tc2_prepare(c))) return rc;
+        std::vector<int> first(L.nblocks), count(L.nblocks, 1);
+        std::iota(first.begin(), first.end(), 0);
+        if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl))) return rc;
+        const long long w = L.tc_list_work[256 + NDG];
+        *launches = (long long)L.tc2_sets.size() - 1;
+        *items = w * nbt;
+        *flop = (double)w * nbt * t2_groups(g.P) * 6.0 * 2.0 * TC_ROWS * T2_N * 16;
+    } else {
+        if ((rc = tc_prepare(c))) return rc;
+        if ((rc = tc_lists(c, NDG, &tl))) return rc;
+        const long long w = L.tc_list_work[NDG];
+        *launches = (long long)L.tc_sets.size() - 1;
+        *items = w * nbt;
+        *flop = (double)w * nbt * 4.0 * 2.0 * TC_ROWS * 16 * (64 + 32);
+    }
+    return DGV_OK;
+}
+
 int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
 {
     const Grid &g = c->grid;
@@ -1234,3 +1271,19 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
 }
 
 }  // namespace dgv
+
+extern "C" int dgv_tc_plan(dgv_ctx *ctx, int32_t nvdf, int64_t *launches, int64_t *items, double *tensor_flop)
+{
+    if (!ctx) return DGV_EINVAL;
+    dgv::Ctx *c = &ctx->c;
+    c->err.clear();
+    DGV_CUDA(c, cudaSetDevice(c->device));
+    long long l = 0, it = 0;
+    double fl = 0.0;
+    int rc = dgv::tc_plan(c, nvdf, &l, &it, &fl);
+    if (rc) return rc;
+    if (launches) *launches = l;
+    if (items) *items = it;
+    if (tensor_flop) *tensor_flop = fl;
+    return DGV_OK;
+}

@@ -79,6 +79,7 @@ struct Layout {
     // device work lists {items, item starts, tile order}, keyed by cells per
     // tile (chunk form) or 256 + cells per tile (block form)
     std::map<int, std::vector<void *>> tc_lists;
+    std::map<int, long long> tc_list_work;  // per key: sum of the items' counts
 };
 void free_layout(Layout &L);
 

@@ -148,6 +148,13 @@ class DGVSolver:
         """Block form: VDF tiles (of up to 128) per CTA, 2 or 1."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCTILES, int(n)))
 
+    def tc_plan(self, nvdf: int):
+        """Launches, work items and issued tensor FLOPs of one tensor-core
+        evaluation of nvdf VDFs in the current form."""
+        l = C.c_int64(); it = C.c_int64(); fl = C.c_double()
+        self._check(self._lib.dgv_tc_plan(self._h, int(nvdf), C.byref(l), C.byref(it), C.byref(fl)))
+        return {"launches": l.value, "items": it.value, "tensor_flop": fl.value}
+
     def set_kernel_timing(self, on: bool):
         """Time the collision kernel's launches with CUDA events on the
         context stream (read back with kernel_stats)."""

@@ -94,6 +94,12 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value);
  * and the number of kernels of this library those calls launched.
  * Synchronises on the recorded events; reset != 0 clears the sums. */
 int dgv_kernel_stats(dgv_ctx *ctx, double *ms, int64_t *launches, int64_t *all_launches, int reset);
+/* No counterpart in the reference (measurement hook): the work plan of one
+ * DGV_PREC_TC evaluation of nvdf VDFs in the current tensor-core form --
+ * kernel launches, work items summed over the VDF tiles, and the FLOPs the
+ * MMAs issue (dense tiles, all split products), for tensor-pipe rooflines.
+ * Builds the device records and work lists if they do not exist yet. */
+int dgv_tc_plan(dgv_ctx *ctx, int32_t nvdf, int64_t *launches, int64_t *items, double *tensor_flop);
 /* N, P = su*sv*sw, number of cells, canonical cell (0-based) */
 int dgv_grid_info(const dgv_ctx *ctx, int64_t *N, int32_t *P, int32_t *Nc, int32_t *ccell);
 /* host copies of nodes_u/_v/_w/_gwts (miscset.f90:1112-1183); any may be NULL */
