@@ -104,3 +104,20 @@ def test_tc2_one_tile_per_cta(c1):
     for k in range(8):
         assert rel_err(q1[k], q64[k]) < TOLTC, k
     assert rel_err(q1, q2) < 1e-9  # same per-row arithmetic, only the CTA split differs
+
+
+def test_tc_plan_matches_launches(c1):
+    """dgv_tc_plan: the launches of one evaluation equal those the kernel
+    timer counts, and the issued tensor work exceeds the algorithmic work
+    (dense tiles, three split products)."""
+    o, s = c1["oracle"], c1["solver"]
+    fs = np.stack([o.maxwellian(1.0, 0.3 * k, 0, 0, 0.8) for k in range(40)])
+    plan = s.tc_plan(40)
+    s.set_kernel_timing(True)
+    s.kernel_stats(reset=True)
+    s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    st = s.kernel_stats(reset=True)
+    s.set_kernel_timing(False)
+    assert st["launches"] == plan["launches"] > 0
+    assert plan["items"] > 0
+    assert plan["tensor_flop"] > 3.0 * s.A_info()["record_shifts"] * 40
