@@ -1200,8 +1200,13 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
     const long long nbt = (nvdf + VB - 1) / VB;
     TcLists tl;
     int rc;
-    if (c->tc_form == 2 && (g.P == 27 || g.P == 8)) {
-        if ((rc = tc2_prepare(c))) return rc;
+    bool block = c->tc_form == 2 && (g.P == 27 || g.P == 8);
+    if (block && (rc = tc2_prepare(c))) {
+        if (rc != DGV_ENOMEM) return rc;
+        c->err.clear();
+        block = false;  // as collide_tc_device: the chunk form serves
+    }
+    if (block) {
         std::vector<int> first(L.nblocks), count(L.nblocks, 1);
         std::iota(first.begin(), first.end(), 0);
         if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl))) return rc;
@@ -1227,7 +1232,13 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
     if (!L.blk) return set_err(c, DGV_ESTATE, "collide: no A-arrays loaded");
     if (g.P > 32) return set_err(c, DGV_EUNSUP, "tensor-core path: at most 32 nodes per cell");
     if (nvdf < 1) return set_err(c, DGV_EINVAL, "collide: batch must hold at least one VDF");
-    if (c->tc_form == 2 && (g.P == 27 || g.P == 8)) return collide_tc2_device(c, d_f, d_q, nvdf, scale);
+    if (c->tc_form == 2 && (g.P == 27 || g.P == 8)) {
+        // the block records need ~2x the room of the chunk records: when they
+        // do not fit, the chunk form serves the call
+        const int rc2 = collide_tc2_device(c, d_f, d_q, nvdf, scale);
+        if (rc2 != DGV_ENOMEM || L.tc2_W) return rc2;
+        c->err.clear();
+    }
     int rc = tc_prepare(c);
     if (rc) return rc;
     rc = ensure_errflag(c);
