@@ -946,7 +946,11 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             // FP32 accumulator, fp16 A and B, both K-major, M = 128, N = 128
+            // the last group holds P*P - 256 (NG-1) columns: its MMAs use
+            // N rounded up to 16, not 256
+            constexpr int NLAST = ((P * P - (NG - 1) * T2_N) + 15) / 16 * 16;
             const uint32_t idesc = (1u << 4) | ((uint32_t)(T2_N >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            const uint32_t idesc_last = (1u << 4) | ((uint32_t)(NLAST >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             int q = 0, gw = 0, J = 0;
             bool ok = true;
             for (int it = i0; it < i1 && ok; it++) {
@@ -957,6 +961,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                     if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err)) { ok = false; break; }
                     const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
                     const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
+                    const uint32_t id = g == NG - 1 ? idesc_last : idesc;
                     for (int j = 0; j < nb2; j++, J++) {
                         const int cs = J & 1;
                         if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
@@ -967,9 +972,9 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                         const uint32_t dacc = tmem + (uint32_t)(cs * T2_N);
 #pragma unroll
                         for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 256 B along K
-                            umma_f16(dacc, dAh + 16 * t, dWh + 16 * t, idesc, t ? 1u : 0u);
-                            umma_f16(dacc, dAh + 16 * t, dWl + 16 * t, idesc, 1u);
-                            umma_f16(dacc, dAl + 16 * t, dWh + 16 * t, idesc, 1u);
+                            umma_f16(dacc, dAh + 16 * t, dWh + 16 * t, id, t ? 1u : 0u);
+                            umma_f16(dacc, dAh + 16 * t, dWl + 16 * t, id, 1u);
+                            umma_f16(dacc, dAl + 16 * t, dWh + 16 * t, id, 1u);
                         }
                         umma_commit(&c_full[cs]);
                     }
@@ -1213,7 +1218,8 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
         const long long w = L.tc_list_work[256 + NDG];
         *launches = (long long)L.tc2_sets.size() - 1;
         *items = w * nbt;
-        *flop = (double)w * nbt * t2_groups(g.P) * 6.0 * 2.0 * TC_ROWS * T2_N * 16;
+        const int ng2 = t2_groups(g.P), nlast = ((g.P * g.P - (ng2 - 1) * T2_N) + 15) / 16 * 16;
+        *flop = (double)w * nbt * ((ng2 - 1) * T2_N + nlast) * 6.0 * 2.0 * TC_ROWS * 16;
     } else {
         if ((rc = tc_prepare(c))) return rc;
         if ((rc = tc_lists(c, NDG, &tl))) return rc;
