@@ -226,6 +226,8 @@ def run_ours(args, world, rank, local):
         solver.set_tc_form(args.tc_form)
     if args.tc_tiles:
         solver.set_tc_tiles_per_cta(args.tc_tiles)
+    if args.tc_set_mb:
+        solver.set_tc_set_mb(args.tc_set_mb)
     t = time.perf_counter()
     solver.generate_synthetic_A(seed=SEED_A, support=1)
     t_gen = time.perf_counter() - t
@@ -541,6 +543,8 @@ def main():
                     help="tensor-core form of the headline arm (0 = the library default)")
     ap.add_argument("--tc-tiles", type=int, default=0, choices=[0, 1, 2],
                     help="block form: VDF tiles per CTA (0 = the library default)")
+    ap.add_argument("--tc-set-mb", type=int, default=0,
+                    help="block form: MB of block records per launch (0 = the library default)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -314,6 +314,11 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
         ctx->c.nchunks_opt = (int)value;
         return DGV_OK;
     case DGV_OPT_KTIMING: ctx->c.ktiming = value != 0; return DGV_OK;
+    case DGV_OPT_TCSETMB:
+        if (value < 1 || value > 4096) return set_err(&ctx->c, DGV_EINVAL, "records per launch must be 1..4096 MB");
+        ctx->c.tc_set_mb = (int)value;
+        release_graphs(&ctx->c);
+        return DGV_OK;
     case DGV_OPT_TCTILES:
         if (value != 1 && value != 2) return set_err(&ctx->c, DGV_EINVAL, "VDF tiles per CTA must be 1 or 2");
         ctx->c.tc_tiles_per_cta = (int)value;

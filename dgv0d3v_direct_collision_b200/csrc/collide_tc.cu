@@ -1056,13 +1056,31 @@ static int tc2_prepare(Ctx *c)
                                                                  g.ccell, (float)L.tc2_vscale,
                                                                  (unsigned char *)L.tc2_W);
     DGV_CUDA(c, cudaGetLastError());
-    // block sets of about 48 MB of records: one launch each
+    return DGV_OK;
+}
+
+// Block sets of about c->tc_set_mb MB of records, one launch each; a changed
+// size drops the block-form work lists built for the old sets.
+static void tc2_sets(Ctx *c)
+{
+    Layout &L = c->lay;
+    if (L.tc2_set_mb == c->tc_set_mb && !L.tc2_sets.empty()) return;
+    for (auto it = L.tc_lists.begin(); it != L.tc_lists.end();) {
+        if (it->first >= 256) {
+            for (void *p : it->second) cudaFree(p);
+            L.tc_list_work.erase(it->first);
+            it = L.tc_lists.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    const long long rec = (long long)t2_groups(c->grid.P) * T2_GREC;
     L.tc2_sets.clear();
     L.tc2_sets.push_back(0);
-    const long long per_set = std::max<long long>(1, (48LL << 20) / (long long)rec);
+    const long long per_set = std::max<long long>(1, ((long long)c->tc_set_mb << 20) / rec);
     for (long long b = per_set; b < L.nblocks; b += per_set) L.tc2_sets.push_back((int)b);
     if (L.tc2_sets.back() != (int)L.nblocks) L.tc2_sets.push_back((int)L.nblocks);
-    return DGV_OK;
+    L.tc2_set_mb = c->tc_set_mb;
 }
 
 template <int VB, int P>
@@ -1100,6 +1118,7 @@ static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, 
     Layout &L = c->lay;
     int rc = tc2_prepare(c);
     if (rc) return rc;
+    tc2_sets(c);
     rc = ensure_errflag(c);
     if (rc) return rc;
     const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), NDG = TC_ROWS / VB;
@@ -1183,6 +1202,7 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
         block = false;  // as collide_tc_device: the chunk form serves
     }
     if (block) {
+        tc2_sets(c);
         std::vector<int> first(L.nblocks), count(L.nblocks, 1);
         std::iota(first.begin(), first.end(), 0);
         if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl))) return rc;

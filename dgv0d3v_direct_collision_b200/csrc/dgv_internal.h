@@ -76,6 +76,7 @@ struct Layout {
     void *tc2_W = nullptr;  // device
     double tc2_vscale = 1.0;
     std::vector<int> tc2_sets;
+    int tc2_set_mb = 0;  // record megabytes per set the sets were built for
     // device work lists {items, item starts, tile order}, keyed by cells per
     // tile (chunk form) or 256 + cells per tile (block form)
     std::map<int, std::vector<void *>> tc_lists;
@@ -131,6 +132,7 @@ struct Ctx {
     bool ktiming = false;
     int tc_form = 2;  // DGV_OPT_TCFORM: 1 chunk form, 2 block form (8 or 27 nodes per cell)
     int tc_tiles_per_cta = 2;  // DGV_OPT_TCTILES: VDF tiles per CTA in the block form
+    int tc_set_mb = 48;        // DGV_OPT_TCSETMB: block form, MB of records per launch
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
     long long kt_launches = 0, kt_all = 0;
     double kt_ms = 0.0;

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (DGVError, GridDesc, DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC, DGV_OPT_PROJECT,
-                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM, DGV_OPT_TCTILES)
+                   DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM, DGV_OPT_TCTILES, DGV_OPT_TCSETMB)
 
 PRECISIONS = {"f64": DGV_PREC_F64, "f32c": DGV_PREC_F32C, "tc": DGV_PREC_TC}
 
@@ -154,6 +154,10 @@ class DGVSolver:
         l = C.c_int64(); it = C.c_int64(); fl = C.c_double()
         self._check(self._lib.dgv_tc_plan(self._h, int(nvdf), C.byref(l), C.byref(it), C.byref(fl)))
         return {"launches": l.value, "items": it.value, "tensor_flop": fl.value}
+
+    def set_tc_set_mb(self, mb: int):
+        """Block form: megabytes of block records per kernel launch."""
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCSETMB, int(mb)))
 
     def set_kernel_timing(self, on: bool):
         """Time the collision kernel's launches with CUDA events on the

@@ -62,6 +62,9 @@ extern "C" {
 #define DGV_OPT_TCTILES 5  /* block form: VDF tiles of 128 per CTA, 2 (one W  */
                            /* read from L2 per 256 rows, one accumulator per  */
                            /* tile) or 1 (two accumulators per tile)          */
+#define DGV_OPT_TCSETMB 6  /* block form: MB of block records per kernel     */
+                           /* launch (default 48; a launch's records are read */
+                           /* by all its CTAs, so they should stay in L2)     */
 
 typedef struct dgv_ctx dgv_ctx;
 

@@ -121,3 +121,20 @@ def test_tc_plan_matches_launches(c1):
     assert st["launches"] == plan["launches"] > 0
     assert plan["items"] > 0
     assert plan["tensor_flop"] > 3.0 * s.A_info()["record_shifts"] * 40
+
+
+def test_tc2_launch_size_option(c1):
+    """DGV_OPT_TCSETMB: more or fewer block records per launch changes the
+    number of launches, not the result."""
+    o, s = c1["oracle"], c1["solver"]
+    fs = np.stack([o.maxwellian(1.0, 0.2 * k, 0, 0, 0.7) for k in range(20)])
+    q48 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    n48 = s.tc_plan(20)["launches"]
+    s.set_tc_set_mb(8)
+    try:
+        q8 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+        n8 = s.tc_plan(20)["launches"]
+    finally:
+        s.set_tc_set_mb(48)
+    assert n8 > n48
+    assert rel_err(q8, q48) < 1e-12
