@@ -137,4 +137,4 @@ def test_tc2_launch_size_option(c1):
     finally:
         s.set_tc_set_mb(48)
     assert n8 > n48
-    assert rel_err(q8, q48) < 1e-12
+    assert rel_err(q8, q48) < 1e-10  # only the grouping of compensated partial sums differs
