@@ -1,5 +1,10 @@
 // collide_tc.cu -- batched Q(f,f) on the 5th-generation tensor cores.
 //
+// Two forms share this file: the chunk form described here (products of
+// f-values formed per pair on the CUDA cores, DGV_OPT_TCFORM = 1) and the
+// block form further down (dense per-block value matrices on the tensor core,
+// the default for 8 or 27 nodes per cell).
+//
 // Per cell-pair block (c1,c2) and output cell D the operator is a product of
 // two small matrices:  Q[(D,b), p] += sum_k  P[(D,b), k] * V[k, p],
 //   P[(D,b), k] = f_b(c1+D-ccell, l1_k) * f_b(c2+D-ccell, l2_k)   (k = pair)
