@@ -58,7 +58,7 @@ def test_two_rank_gather_and_max():
     import torch.multiprocessing as mp
     port = _free_port()
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this (threaded) process
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     assert out[0] == 0.0 and out[1] == 0.0  # bit-identical assembly
@@ -104,7 +104,7 @@ def test_two_rank_sharded_rk_step():
     stage, reproduces the unsplit RK4 step."""
     import torch.multiprocessing as mp
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this (threaded) process
     out = mgr.dict()
     mp.spawn(_rk_worker, args=(2, port, out), nprocs=2, join=True)
     assert out[0] < 1e-12 and out[1] < 1e-12
