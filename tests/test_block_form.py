@@ -59,3 +59,44 @@ def test_block_form_equals_oracle(s, M, L, seed):
     # the blocks are dense enough that the W matrices are the sensible unit
     fill = np.mean([np.count_nonzero(W.any(axis=2)) / (P * P) for W in blocks.values()])
     assert 0.0 < fill <= 1.0
+
+
+@pytest.mark.parametrize("s,M,L,seed", [(2, 3, 3.0, 5)])
+def test_block_form_adjoint_equals_oracle_vjp(s, M, L, seed):
+    """The adjoint in the same block form: with c = 2 v / w per output node,
+    g(c1 + D, l1) += sum_p c[D, p] G[D, l1, p]   (G = F2 W, the forward's
+    tensor-core product) and g(c2 + D, l2) += (W (f1 x c))[l2], both scattered
+    to the shifted cells.  Equals the oracle's VJP (the adjoint of
+    collision_mod.f90:213-216) to 1e-13."""
+    from oracle.oracle import Oracle
+    o = Oracle(s, M, L)
+    cap, A, xi, xi1 = o.synth_A(seed=seed, support=1)
+    o.set_A(cap, A, xi, xi1)
+    P, Nc = o.P, o.Nc
+    p = np.repeat(np.arange(o.N), cap) % P
+    blocks = {}
+    for k in range(len(A)):
+        W = blocks.setdefault((int(xi[k] // P), int(xi1[k] // P)), np.zeros((P, P, P)))
+        W[xi1[k] % P, xi[k] % P, p[k]] += A[k]
+    rng = np.random.default_rng(seed)
+    f = o.maxwellian(0.7, 0.4, 0.1, -0.2, 0.9) * (1.0 + 0.05 * rng.standard_normal(o.N))
+    v = rng.standard_normal(o.N)
+    fc = f.reshape(Nc, P)
+    cq = (2.0 * v / o.gwts).reshape(Nc, P)
+    cc = _cell3(np.array(o.ccell), M)
+    D3 = _cell3(np.arange(Nc), M)
+    g = np.zeros((Nc, P))
+    for (a, b), W in blocks.items():
+        s1 = _cell3(np.array(a), M) + D3 - cc
+        s2 = _cell3(np.array(b), M) + D3 - cc
+        ok = np.all((s1 >= 0) & (s1 < M) & (s2 >= 0) & (s2 < M), axis=1)
+        if not ok.any():
+            continue
+        i1 = (s1[ok, 0] * M + s1[ok, 1]) * M + s1[ok, 2]
+        i2 = (s2[ok, 0] * M + s2[ok, 1]) * M + s2[ok, 2]
+        G = np.einsum("dk,klp->dlp", fc[i2], W)
+        np.add.at(g, i1, np.einsum("dlp,dp->dl", G, cq[ok]))
+        np.add.at(g, i2, np.einsum("klp,dl,dp->dk", W, fc[i1], cq[ok]))
+    g = g.ravel()
+    ref = o.vjp(f, v)
+    assert np.linalg.norm(g - ref) / np.linalg.norm(ref) < 1e-13
