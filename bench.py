@@ -137,6 +137,16 @@ def barrier(world):
         dist.barrier()
 
 
+def balanced_cells(Mc: int):
+    """The M^2 cells (u, v, w) of an M^3 grid with (u + 2v + 4w) mod M == 0
+    (M odd): every (u, v) once, every w value M times, so boundary and
+    interior cells (whose per-node cost differs by the number of valid
+    shifts) appear in their grid proportions; in a seeded random order."""
+    cells = [(u * Mc + v) * Mc + w for u in range(Mc) for v in range(Mc) for w in range(Mc)
+             if (u + 2 * v + 4 * w) % Mc == 0]
+    return np.random.default_rng(0).permutation(np.array(cells))
+
+
 class CpuBaseline:
     """Oracle (CPU restatement of EvalCollisionPeriodicAPlus_DGV) on a sample
     of output nodes of the same workload.  All nodes scan the same record
@@ -152,30 +162,60 @@ class CpuBaseline:
         self.o.set_A(cap, A, xi, xi1)
         self.f = mixture_batch(self.o.u, self.o.v, self.o.w, self.o.gwts, 1, 7)[0]
         self.cores = nthreads or os.cpu_count()
-        cells = np.random.default_rng(0).permutation(self.o.Nc)
-        self.nodes_all = cells * self.o.P + self.P_SAMPLE
+        self.nodes_all = balanced_cells(M) * self.o.P + self.P_SAMPLE
         self.n = None
 
     def sample(self, seconds_target: float = 15.0):
         o = self.o
-        if self.n is None:  # size the sample from a short probe
-            n0 = min(o.Nc, max(self.cores, 8))
+        nall = len(self.nodes_all)
+        if self.n is None:  # size the sample from a short probe: whole rounds of the threads
+            n0 = min(nall, max(self.cores, 8))
             t = time.perf_counter()
             o.collide(self.f, nodes=self.nodes_all[:n0], nthreads=self.cores)
             dt0 = time.perf_counter() - t
-            self.n = int(min(o.Nc, max(n0, seconds_target / max(dt0 / n0, 1e-9))))
+            n = int(min(nall, max(n0, seconds_target / max(dt0 / n0, 1e-9))))
+            # whole rounds of the threads: a partial last round would leave
+            # threads idle and overstate the time per node
+            self.n = max(min(nall, self.cores), n // self.cores * self.cores)
         t = time.perf_counter()
         o.collide(self.f, nodes=self.nodes_all[:self.n], nthreads=self.cores)
         dt1 = time.perf_counter() - t
         eval_s = dt1 / self.n * o.N
         return {"value": 1.0 / eval_s, "unit": "evals/s", "cores": self.cores, "kind": "port",
                 "sample": f"{self.n} of {o.N} output nodes of one 27^3 VDF (records of basis function "
-                          f"{self.P_SAMPLE}, cells in a seeded random order), {dt1:.1f} s; full evaluation = "
-                          f"time per node x N"}, dt1
+                          f"{self.P_SAMPLE}, cells of a balanced sample of {nall}), {dt1:.1f} s; full evaluation "
+                          f"= time per node x N"}, dt1
+
+
+def calibrate_sampling(nthreads: int = 0):
+    """Checks the node-sample estimate against a full evaluation where one is
+    cheap: the 15^3 grid (s=3, M=5, [-6,6]^3, all 27 basis functions' synthetic
+    records), one seeded mixture VDF.  The full oracle evaluation is timed once,
+    and the estimate the 27^3 baseline uses (records of basis function 13 only,
+    a node sample of that basis function, time per node x N) beside it."""
+    from oracle.oracle import Oracle
+    cores = nthreads or os.cpu_count()
+    o = Oracle(3, 5, 6.0)
+    f = mixture_batch(o.u, o.v, o.w, o.gwts, 1, 7)[0]
+    o.set_A(*o.synth_A(seed=SEED_A, support=1))
+    t = time.perf_counter()
+    o.collide(f, nthreads=cores)
+    full = time.perf_counter() - t
+    # the estimator of the 27^3 baseline: balanced cells, whole rounds of the
+    # threads, time per node x N (three basis functions here, for enough nodes)
+    cand = np.array([c * o.P + p for c in balanced_cells(5) for p in (CpuBaseline.P_SAMPLE, 4, 22)])
+    nodes = cand[:max(cores, len(cand) // cores * cores)]
+    t = time.perf_counter()
+    o.collide(f, nodes=nodes, nthreads=cores)
+    est = (time.perf_counter() - t) / len(nodes) * o.N
+    return {"grid": "15^3 (s=3, M=5, [-6,6]^3), one VDF", "full_s": full, "estimated_s": est,
+            "estimate_over_full": est / full, "sample_nodes": int(len(nodes)), "cores": cores}
 
 
 def cpu_baseline(seconds_target: float = 15.0, nthreads: int = 0):
-    return CpuBaseline(nthreads).sample(seconds_target)
+    res, dt = CpuBaseline(nthreads).sample(seconds_target)
+    res["calibration"] = calibrate_sampling(nthreads)
+    return res, dt
 
 
 def run_reference(args, world, rank):
@@ -191,6 +231,7 @@ def run_reference(args, world, rank):
             res = r
     val = 1.0 / statistics.mean(times)
     res["value"] = val
+    res["calibration"] = calibrate_sampling()
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "evals/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / val,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -310,6 +351,37 @@ def run_ours(args, world, rank, local):
     ms_e2e = max_over_ranks(e0.elapsed_time(e1), world)
     e2e = world * BATCH * args.steps / (ms_e2e / 1000.0)
 
+    # adjoint (vector-Jacobian product) of the same batch on the tensor cores,
+    # cotangents v ~ N(0,1) per node; its time per batch against the forward's
+    # (one batched evaluation with the projection, timed above); error against
+    # the FP64 device VJP on two VDFs
+    adjoint = None
+    if args.adjoint_steps > 0:
+        v_dev = torch.tensor(np.random.default_rng(2000 + rank).standard_normal(fb.shape), device=f_dev.device)
+        g_dev = torch.empty_like(f_dev)
+        with torch.cuda.stream(stream):
+            t = time.perf_counter()
+            solver.vjp(f_dev, v_dev, g_dev, precision="tc")  # builds the adjoint's block records and lists
+            torch.cuda.synchronize()
+            t_adj = time.perf_counter() - t
+            solver.vjp(f_dev, v_dev, g_dev, precision="tc")
+            torch.cuda.synchronize()
+            barrier(world)
+            e0.record(stream)
+            for _ in range(args.adjoint_steps):
+                solver.vjp(f_dev, v_dev, g_dev, precision="tc")
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms_adj = max_over_ranks(e0.elapsed_time(e1), world) / args.adjoint_steps
+        g64 = solver.vjp(f_dev[:2].contiguous(), v_dev[:2].contiguous(), precision="f64").cpu().numpy()
+        gtc = g_dev[:2].cpu().numpy()
+        aerr = float(max(np.linalg.norm(gtc[k] - g64[k]) / np.linalg.norm(g64[k]) for k in range(2)))
+        adjoint = {"ms_per_batch": ms_adj, "evals_per_s": world * BATCH / (ms_adj / 1000.0),
+                   "adjoint_over_forward": ms_adj / (ms_max / args.steps), "steps": args.adjoint_steps,
+                   "err_tc_vs_f64_vjp_norm_max": aerr, "setup_s": t_adj,
+                   "form": "block form: G = f(c2) W1 and f(c1) W2 per cell-pair block on the tensor cores, "
+                           "contracted with c = 2v/w; target-cell ownership"}
+
     if rank != 0:
         return
     try:
@@ -362,6 +434,7 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": None,
         "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": int(BATCH * N * 8),
                 "d2h_bytes_per_step": int(BATCH * N * 8)},
+        "adjoint": adjoint,
         "gpu_launches": int(kst["all_launches"]),
         "clocks": clk.summary(),
         "setup_s": {"synthetic_A": t_gen, "tensor_core_layout_and_lists": t_prep},
@@ -489,7 +562,8 @@ def run_profile_case(case: str):
     tuning launches) for the CUDA-core kernels, a batch of 256 VDFs for the
     tensor-core kernels (one launch per block set; "tc" the chunk form, "tc2"
     the block form).  "<prec>_15": the 15^3 grid (s=3, M=5, [-6,6]^3; rows
-    ~0.6 GB), 256 VDFs.  "<prec>_27": the benchmark workload itself (27^3 x
+    ~0.6 GB), 256 VDFs ("vjptc": the tensor-core adjoint with v = f; "f64":
+    one VDF).  "<prec>_27": the benchmark workload itself (27^3 x
     256 VDFs), for single-pass counters only.  Two evaluations each: a
     warm-up, then the one to capture."""
     import torch
@@ -502,9 +576,9 @@ def run_profile_case(case: str):
     if prec == "tc2":
         s.set_tc_form(2)
         prec = "tc"
-    if prec != "tc":
+    if prec not in ("tc", "vjptc"):
         s.set_nchunks(296)
-    nb = BATCH if prec == "tc" else 1
+    nb = BATCH if prec in ("tc", "vjptc") else 1
     fb = mixture_batch(s.nodes_u, s.nodes_v, s.nodes_w, s.nodes_gwts, nb, 3)
     f = torch.tensor(fb if nb > 1 else fb[0], dtype=torch.float64, device="cuda")
     q = torch.empty_like(f)
@@ -513,6 +587,8 @@ def run_profile_case(case: str):
         t = time.perf_counter()
         if prec == "vjp":
             s.vjp(f, f, q)
+        elif prec == "vjptc":
+            s.vjp(f, f, q, precision="tc")
         else:
             s.EvalCollisionPeriodicAPlus_DGV(f, q, precision=prec)
         torch.cuda.synchronize()
@@ -523,7 +599,7 @@ def run_profile_case(case: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile-case", choices=["f64_21", "f32c_21", "vjp_21", "tc_21", "tc_27", "tc2_21", "tc2_27",
-                                               "tc_15", "tc2_15"],
+                                               "tc_15", "tc2_15", "vjptc_15", "vjptc_27", "f64_15"],
                     default=None,
                     help="small single-VDF case for profiler captures (no JSON bench line)")
     ap.add_argument("--gpus", type=int, default=1)
@@ -543,6 +619,8 @@ def main():
                     help="tensor-core form of the headline arm (0 = the library default)")
     ap.add_argument("--tc-tiles", type=int, default=0, choices=[0, 1, 2],
                     help="block form: VDF tiles per CTA (0 = the library default)")
+    ap.add_argument("--adjoint-steps", type=int, default=3,
+                    help="timed tensor-core VJP evaluations of the batch (0 = skip the adjoint)")
     ap.add_argument("--tc-set-mb", type=int, default=0,
                     help="block form: MB of block records per launch (0 = the library default)")
     args = ap.parse_args()

@@ -25,7 +25,7 @@ EXPORTS = [
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper", "dgv_set_regime",
     "dgv_regime_info",
     "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
-    "dgv_jvp", "dgv_vjp", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
+    "dgv_jvp", "dgv_vjp", "dgv_vjp_batched", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
     "dgv_compute_A", "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
     "dgv_write_solution", "dgv_read_solution", "dgv_write_solution_arrays", "dgv_read_solution_arrays",
     "dgv_collide_group", "dgv_tc_plan",
@@ -98,6 +98,7 @@ def load() -> C.CDLL:
         "dgv_project": [vp, vp, i32],
         "dgv_jvp": [vp, vp, vp, vp, C.c_int],
         "dgv_vjp": [vp, vp, vp, vp, C.c_int],
+        "dgv_vjp_batched": [vp, i32, vp, vp, vp, C.c_int],
         "dgv_prepare_linear": [vp, vp],
         "dgv_apply_linear": [vp, vp, vp, C.c_int],
         "dgv_collide_f64_noalloc": [vp, vp, vp, i32, vp],

@@ -129,7 +129,7 @@ typedef void (*VjpFn)(VjpArgs);
 
 int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int precision)
 {
-    (void)precision;
+    if (precision != DGV_PREC_F64) return set_err(c, DGV_EUNSUP, "vjp: this kernel computes in FP64 only");
     if (!c->lay.blk) return set_err(c, DGV_ESTATE, "vjp: no A-arrays loaded");
     const Grid &g = c->grid;
     const Layout &L = c->lay;

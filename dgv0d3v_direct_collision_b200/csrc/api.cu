@@ -64,17 +64,27 @@ int check_errflag(Ctx *c)
     return DGV_OK;
 }
 
-static bool is_device_ptr(const void *p)
+// Where an array lives: *dev = true for memory of the context's device (or
+// managed memory), false for host memory; device memory of another GPU is
+// refused (a kernel of this context cannot read it safely).
+int classify_ptr(Ctx *c, const void *p, bool *dev)
 {
     cudaPointerAttributes at;
+    *dev = false;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return DGV_OK;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    if (at.type == cudaMemoryTypeManaged) {
+        *dev = true;
+    } else if (at.type == cudaMemoryTypeDevice) {
+        if (at.device != c->device)
+            return set_err(c, DGV_EINVAL, "an array lives on device " + std::to_string(at.device) +
+                                              ", the context on device " + std::to_string(c->device));
+        *dev = true;
+    }
+    return DGV_OK;
 }
-
-bool is_device_pointer(const void *p) { return is_device_ptr(p); }
 
 // Inverse of the Gram matrix G_ab = sum_i w_i psi_a psi_b of the invariants
 static int gram_inverse(Ctx *c)
@@ -191,8 +201,11 @@ static int reserve_in(Ctx *c, size_t need_doubles)
 
 static int stage_in(Ctx *c, const double *p, size_t n, size_t slot, const double **d)
 {
-    if (is_device_ptr(p)) { *d = p; return DGV_OK; }
-    int rc = reserve_in(c, slot + n);
+    bool dev = false;
+    int rc = classify_ptr(c, p, &dev);
+    if (rc) return rc;
+    if (dev) { *d = p; return DGV_OK; }
+    rc = reserve_in(c, slot + n);
     if (rc) return rc;
     DGV_CUDA(c, cudaMemcpyAsync(c->d_in + slot, p, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     *d = c->d_in + slot;
@@ -201,8 +214,11 @@ static int stage_in(Ctx *c, const double *p, size_t n, size_t slot, const double
 
 static int out_ptr(Ctx *c, double *p, size_t n, double **d, bool *host)
 {
-    if (is_device_ptr(p)) { *d = p; *host = false; return DGV_OK; }
-    int rc = ensure_buffer(c, &c->d_out, &c->out_bytes, n * sizeof(double));
+    bool dev = false;
+    int rc = classify_ptr(c, p, &dev);
+    if (rc) return rc;
+    if (dev) { *d = p; *host = false; return DGV_OK; }
+    rc = ensure_buffer(c, &c->d_out, &c->out_bytes, n * sizeof(double));
     if (rc) return rc;
     *d = c->d_out;
     *host = true;
@@ -276,6 +292,7 @@ int dgv_ctx_create(const dgv_grid_desc *desc, int device, dgv_ctx **out)
         delete h;
         return DGV_ECUDA;
     }
+    noalloc_prepare(c);
     *out = h;
     return DGV_OK;
 }
@@ -516,8 +533,10 @@ int dgv_step_rk(dgv_ctx *ctx, double *f, double *frhs1, double dt, int order, in
     Ctx *c = &ctx->c;
     if (!f) return set_err(c, DGV_EINVAL, "step_rk: NULL f");
     size_t n = (size_t)c->grid.N;
-    bool fdev = is_device_ptr(f);
-    bool rhost = frhs1 && !is_device_ptr(frhs1);
+    bool fdev = false, rdev = false;
+    TRY(classify_ptr(c, f, &fdev));
+    if (frhs1) TRY(classify_ptr(c, frhs1, &rdev));
+    bool rhost = frhs1 && !rdev;
     if (!fdev || rhost) TRY(ensure_buffer(c, &c->d_out, &c->out_bytes, 2 * n * sizeof(double)));
     double *df = fdev ? f : c->d_out;
     double *dr = rhost ? c->d_out + n : frhs1;
@@ -538,7 +557,8 @@ static int ab_common(dgv_ctx *ctx, double *f, double dt, int order, int precisio
     Ctx *c = &ctx->c;
     if (!f) return set_err(c, DGV_EINVAL, "AB: NULL f");
     size_t n = (size_t)c->grid.N;
-    bool fdev = is_device_ptr(f);
+    bool fdev = false;
+    TRY(classify_ptr(c, f, &fdev));
     double *df = f;
     if (!fdev) {
         TRY(ensure_buffer(c, &c->d_out, &c->out_bytes, n * sizeof(double)));
@@ -593,7 +613,8 @@ int dgv_project(dgv_ctx *ctx, double *q, int32_t nb)
     Ctx *c = &ctx->c;
     if (!q || nb < 1) return set_err(c, DGV_EINVAL, "project: need nb >= 1 and a non-NULL array");
     size_t n = (size_t)nb * (size_t)c->grid.N;
-    bool dev = is_device_ptr(q);
+    bool dev = false;
+    TRY(classify_ptr(c, q, &dev));
     double *dq = q;
     if (!dev) {
         TRY(ensure_buffer(c, &c->d_out, &c->out_bytes, n * sizeof(double)));
@@ -623,10 +644,17 @@ int dgv_jvp(dgv_ctx *ctx, const double *f, const double *df, double *q, int prec
 
 int dgv_vjp(dgv_ctx *ctx, const double *f, const double *v, double *g, int precision)
 {
+    return dgv_vjp_batched(ctx, 1, f, v, g, precision);
+}
+
+int dgv_vjp_batched(dgv_ctx *ctx, int32_t nb, const double *f, const double *v, double *g, int precision)
+{
     CTX_CHECK(ctx);
     Ctx *c = &ctx->c;
-    if (!f || !v || !g) return set_err(c, DGV_EINVAL, "vjp: NULL array");
-    size_t n = (size_t)c->grid.N;
+    if (!f || !v || !g || nb < 1) return set_err(c, DGV_EINVAL, "vjp: need nb >= 1 and non-NULL arrays");
+    if (precision != DGV_PREC_F64 && precision != DGV_PREC_TC)
+        return set_err(c, DGV_EUNSUP, "vjp: FP64 (DGV_PREC_F64) or tensor cores (DGV_PREC_TC) only");
+    const size_t N = (size_t)c->grid.N, n = (size_t)nb * N;
     const double *d1, *d2;
     double *dg;
     bool host = false;
@@ -634,7 +662,11 @@ int dgv_vjp(dgv_ctx *ctx, const double *f, const double *v, double *g, int preci
     TRY(stage_in(c, f, n, 0, &d1));
     TRY(stage_in(c, v, n, n, &d2));
     TRY(out_ptr(c, g, n, &dg, &host));
-    TRY(vjp_device(c, d1, d2, dg, precision));
+    if (precision == DGV_PREC_TC) {
+        TRY(vjp_tc_device(c, d1, d2, dg, nb));
+    } else {
+        for (int32_t b = 0; b < nb; b++) TRY(vjp_device(c, d1 + b * N, d2 + b * N, dg + b * N, precision));
+    }
     return finish(c, g, dg, n, host);
 }
 

@@ -428,7 +428,7 @@ int collide_cells_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int p
 int jvp_device(Ctx *c, const double *d_f, const double *d_df, double *d_q, int precision)
 {
     if (!c->lay.blk) return set_err(c, DGV_ESTATE, "jvp: no A-arrays loaded");
-    (void)precision;
+    if (precision != DGV_PREC_F64) return set_err(c, DGV_EUNSUP, "jvp: the mixed-terms kernel computes in FP64 only");
     int nch = choose_chunks(c, d_f, d_df, d_q, 1, DGV_PREC_F64, 0, c->grid.Nc);
     // the bilinear kernel sums 2/w * A * (f g + g f) / 2 * 2: the reduce
     // kernel's factor 2 is the reference's "2*fc/w" (collision_mod.f90:326)

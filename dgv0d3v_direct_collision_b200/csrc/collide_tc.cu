@@ -517,7 +517,7 @@ __global__ void k_absmax_rows(const double *rows64, long long npairs, int RD64, 
 // per-VDF scale 2^e (max |f| -> [32, 64)) and the scaled copy of f in VDF
 // tiles of VB: F[((bt*Nc + cell)*P + l)*VB + v%VB]
 __global__ void k_tc_fprep(const double *f, long long N, int nvdf, double vinv, float *F, double *inv_scale,
-                           int Nc, int P, int VB)
+                           int Nc, int P, int VB, int pw)
 {
     const int v = blockIdx.x;
     __shared__ double red[32];
@@ -540,7 +540,7 @@ __global__ void k_tc_fprep(const double *f, long long N, int nvdf, double vinv, 
         e = 6 - e;
     }
     const double s = ldexp(1.0, e);
-    if (threadIdx.x == 0) inv_scale[v] = ldexp(1.0, -2 * e) * vinv;
+    if (threadIdx.x == 0) inv_scale[v] = ldexp(1.0, -pw * e) * vinv;  // f enters the result pw times
     const int bt = v / VB, lb = v % VB;
     for (long long i = threadIdx.x; i < N; i += blockDim.x) {
         const int cell = (int)(i / P), l = (int)(i - (long long)cell * P);
@@ -633,8 +633,52 @@ struct TcLists {
     int *tile_of = nullptr;     // per set: ntiles entries
 };
 
+// Adds the items of one block for one owner-cell shift: every output cell D
+// of the block's box maps to the owner cell T = D + shift (linear indices;
+// exact, the box keeps both shifted cells inside the grid); owner cells of a
+// tile are consecutive, so an item is pushed once per (tile, id) and the
+// owner cells it serves are set as bits.
+// An item's nch holds `low` (chunk form: its chunk records; block form: the
+// block's mask of nodes l1) and the owner-cell bits from bit `vshift` (16 in
+// the chunk form, 27 in the block form); `weight` is its work for the tile
+// ordering and the plan.
+static void tc_items_for_block(const Grid &g, const BlockInfo &bi, int NDG, int shift, int id, int low, int vshift,
+                               long long weight, int fc1, int fc2, std::vector<std::vector<TcItem>> &per,
+                               std::vector<long long> &work)
+{
+    int last = -1;
+    for (int u = bi.lo[0]; u <= bi.hi[0]; u++)
+        for (int v = bi.lo[1]; v <= bi.hi[1]; v++)
+            for (int w = bi.lo[2]; w <= bi.hi[2]; w++) {
+                const int T = (u * g.d.Mv + v) * g.d.Mw + w + shift, grp = T / NDG;
+                if (grp != last) {  // same tile as the last cell or new
+                    if (per[grp].empty() || per[grp].back().chunk0 != id) {
+                        per[grp].push_back(TcItem{id, low, fc1, fc2});
+                        work[grp] += weight;
+                    }
+                    last = grp;
+                }
+                per[grp].back().nch |= 1 << (vshift + T % NDG);
+            }
+}
+
+constexpr int T2_N_ = 256;  // column group width of the block form (T2_N below)
+
+// columns the MMAs of one block-form item issue: groups of 256, the last
+// rounded up to 16
+__host__ __device__ inline int t2_issued_cols(int ncol)
+{
+    const int ng = (ncol + T2_N_ - 1) / T2_N_;
+    return (ng - 1) * T2_N_ + ((ncol - (ng - 1) * T2_N_) + 15) / 16 * 16;
+}
+
+// mode 0: items of the chunk form (owner = output cell D; first/count = the
+// blocks' chunk records); mode 1: items of the block form's collision
+// operator (owner = output cell D; chunk0 = the block's first record group,
+// nch = its mask of nodes l1); mode 2: items of the block-form adjoint (owner
+// = target cell T, two scatters per block, see k_collide_tc2)
 static int tc_work_lists(Ctx *c, int NDG, int key, const std::vector<int> &sets, const std::vector<int> &first,
-                         const std::vector<int> &count, TcLists *out)
+                         const std::vector<int> &count, TcLists *out, int mode = 0)
 {
     Layout &L = c->lay;
     auto it = L.tc_lists.find(key);
@@ -650,26 +694,29 @@ static int tc_work_lists(Ctx *c, int NDG, int key, const std::vector<int> &sets,
     std::vector<int> start((size_t)nsets * (ng + 1)), tile_of((size_t)nsets * ng);
     std::vector<std::vector<TcItem>> per(ng);
     std::vector<long long> work(ng);
+    long long wsum = 0;
     for (int s = 0; s < nsets; s++) {
         for (auto &v : per) v.clear();
         std::fill(work.begin(), work.end(), 0);
         for (int b = sets[s]; b < sets[s + 1]; b++) {
             const BlockInfo &bi = L.h_blk[b];
-            int last = -1;
-            for (int u = bi.lo[0]; u <= bi.hi[0]; u++)
-                for (int v = bi.lo[1]; v <= bi.hi[1]; v++)
-                    for (int w = bi.lo[2]; w <= bi.hi[2]; w++) {
-                        const int D = (u * g.d.Mv + v) * g.d.Mw + w, grp = D / NDG;
-                        if (grp != last) {  // cells of one tile are consecutive: same tile as the last cell or new
-                            if (per[grp].empty() || per[grp].back().chunk0 != first[b]) {
-                                per[grp].push_back(TcItem{first[b], count[b], bi.c1, bi.c2});
-                                work[grp] += count[b];
-                            }
-                            last = grp;
-                        }
-                        per[grp].back().nch |= 1 << (16 + D % NDG);
-                    }
+            if (mode == 0) {
+                tc_items_for_block(g, bi, NDG, 0, first[b], count[b], 16, count[b], bi.c1, bi.c2, per, work);
+            } else if (mode == 1) {
+                const int msk = (int)L.tc2_mask[b];
+                tc_items_for_block(g, bi, NDG, 0, (int)L.tc2_goff[b], msk, 27,
+                                   t2_issued_cols(__builtin_popcount(msk) * g.P), bi.c1, bi.c2, per, work);
+            } else {
+                const int o1 = bi.c1 - g.ccell, o2 = bi.c2 - g.ccell, full = (1 << g.P) - 1;
+                const long long wcol = t2_issued_cols(g.P * g.P);
+                // pass 1 (W1, to the c1 side): side cells T - o1, F16 cells T - o1 + o2
+                tc_items_for_block(g, bi, NDG, o1, b, full, 27, wcol, g.ccell - o1, g.ccell + o2 - o1, per, work);
+                // pass 2 (W2, to the c2 side): side cells T - o2, F16 cells T - o2 + o1
+                tc_items_for_block(g, bi, NDG, o2, b | (1 << 30), full, 27, wcol, g.ccell - o2, g.ccell + o1 - o2,
+                                   per, work);
+            }
         }
+        for (long long wv : work) wsum += wv;
         int *o = tile_of.data() + (size_t)s * ng;
         std::iota(o, o + ng, 0);
         std::stable_sort(o, o + ng, [&](int x, int y) { return work[x] > work[y]; });
@@ -689,9 +736,8 @@ static int tc_work_lists(Ctx *c, int NDG, int key, const std::vector<int> &sets,
     DGV_CUDA(c, cudaMemcpy(d[1], start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
     DGV_CUDA(c, cudaMemcpy(d[2], tile_of.data(), sizeof(int) * tile_of.size(), cudaMemcpyHostToDevice));
     L.tc_lists[key] = {d[0], d[1], d[2]};
-    long long wsum = 0;
-    for (const TcItem &e : items) wsum += e.nch & 0xffff;
     L.tc_list_work[key] = wsum;
+    L.tc_list_items[key] = (long long)items.size();
     out->items = reinterpret_cast<TcItem *>(d[0]);
     out->item_start = reinterpret_cast<int *>(d[1]);
     out->tile_of = reinterpret_cast<int *>(d[2]);
@@ -747,6 +793,14 @@ constexpr int T2_THREADS = 32 * (2 + T2_EPI_WARPS);
 
 __host__ __device__ constexpr int t2_groups(int P) { return (P * P + T2_N - 1) / T2_N; }
 
+// column groups of a collision-operator item: its block's mask of nodes l1
+// is in the low 27 bits of nch
+template <int P>
+__device__ __forceinline__ int t2_item_groups(int nch)
+{
+    return (__popc((unsigned)nch & 0x7ffffffu) * P + T2_N - 1) / T2_N;
+}
+
 // byte offset of element (row, k) of a K-major tile without swizzle, K = 32:
 // core matrices of 8 rows x 16 bytes, four along K (128 B apart), row groups
 // of 8 512 B apart
@@ -755,14 +809,43 @@ __host__ __device__ __forceinline__ int t2_off(int row, int k)
     return ((row >> 3) * 4 + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-// one record per block: t2_groups(P) groups of {W hi tile, W lo tile}, group
-// g holding columns n = l1*P + p in [128 g, 128 g + 128) as tile rows
-__global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64, int P, int Nc, int ccell,
-                            float vscale, unsigned char *W)
+// per block the mask of the nodes l1 its pairs use (bit l1)
+__global__ void k_tc2_mask(const BlockInfo *blk, const double *rows64, int RD64, int Nc, int ccell, unsigned *mask)
 {
-    const int NG = t2_groups(P);
     const BlockInfo bi = blk[blockIdx.x];
-    unsigned char *rec = W + (size_t)blockIdx.x * NG * T2_GREC;
+    unsigned m = 0u;
+    for (int k = threadIdx.x; k < bi.count; k += blockDim.x) {
+        const long long o = __double_as_longlong(rows64[(size_t)(bi.start + k) * RD64]);
+        const int o1 = (int)(unsigned)(o & 0xffffffffLL);
+        m |= 1u << ((o1 - (bi.c1 - ccell)) / Nc);
+    }
+    m = __reduce_or_sync(0xffffffffu, m);
+    __shared__ unsigned sm[32];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned r = 0u;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r |= sm[w];
+        mask[blockIdx.x] = r;
+    }
+}
+
+// one record per block: t2_groups(P) groups of {W hi tile, W lo tile}, group
+// g holding columns n in [256 g, 256 g + 256) as tile rows.  Arrangement
+// 0 (collision operator): n = l1*P + p, K = l2.  The adjoint's: 1 (to the c1
+// side) n = p*P + l1, K = l2; 2 (to the c2 side) n = p*P + l2, K = l1.
+//
+// Arrangement 0 is compacted: only the nodes l1 of the block's mask get
+// columns, n = j*P + p with j = the rank of l1 in the mask, and the block's
+// record holds goff[b+1] - goff[b] = ceil(popc(mask) P / 256) groups from
+// group goff[b] on.  The adjoint's arrangements keep all P*P columns.
+__global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64, int P, int Nc, int ccell,
+                            float vscale, unsigned char *W, int arr, const unsigned *mask, const long long *goff)
+{
+    const BlockInfo bi = blk[blockIdx.x];
+    const int NG = arr == 0 ? (int)(goff[blockIdx.x + 1] - goff[blockIdx.x]) : t2_groups(P);
+    const unsigned msk = arr == 0 ? mask[blockIdx.x] : 0u;
+    unsigned char *rec = W + (arr == 0 ? (size_t)goff[blockIdx.x] : (size_t)blockIdx.x * NG) * T2_GREC;
     uint4 *r4 = reinterpret_cast<uint4 *>(rec);
     for (int t = threadIdx.x; t < NG * T2_GREC / 16; t += blockDim.x) r4[t] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
@@ -772,11 +855,13 @@ __global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64
         const long long o = __double_as_longlong(row[0]);
         const int o1 = (int)(unsigned)(o & 0xffffffffLL), o2 = (int)(o >> 32);
         const int l1 = (o1 - (bi.c1 - ccell)) / Nc, l2 = (o2 - (bi.c2 - ccell)) / Nc;
-        const int n = l1 * P + p, g = n / T2_N;
+        const int lk = arr == 2 ? l1 : l2;
+        const int n = arr == 0 ? __popc(msk & ((1u << l1) - 1u)) * P + p : p * P + (arr == 2 ? l2 : l1);
+        const int g = n / T2_N;
         const float x = (float)(row[1 + p] * (double)vscale);
         const __half h = __float2half_rn(x);
         const __half l = __float2half_rn(x - __half2float(h));
-        unsigned char *dst = rec + (size_t)g * T2_GREC + t2_off(n - g * T2_N, l2);
+        unsigned char *dst = rec + (size_t)g * T2_GREC + t2_off(n - g * T2_N, lk);
         *reinterpret_cast<__half *>(dst) = h;
         *reinterpret_cast<__half *>(dst + T2_TILE) = l;
     }
@@ -806,10 +891,11 @@ __global__ void k_tc2_f16(const float *F, unsigned char *F16, int nbt, int Nc, i
 }
 
 struct Tc2Args {
-    const float *F;            // [nbt][Nc][P][VB] scaled f, zero for padded VDFs
+    const float *F;            // [nbt][Nc][P][VB] FP32 side factor: scaled f (forward) or c = 2v/w (adjoint)
     const unsigned char *F16;  // [nbt][hi, lo][Nc][VB x 32 tile]
     const unsigned char *W;    // block records
-    const TcItem *items;       // work lists of this launch (chunk0 = block index)
+    const unsigned char *W2;   // adjoint: records W2 (items with 1 << 30); W holds W1
+    const TcItem *items;       // work lists of this launch (chunk0 = block index, | 1 << 30 for W2)
     const int *item_start;     // [ntiles + 1]
     const int *tile_of;        // row-tile index in launch order
     double *qacc;              // [(D*P+p)*NV + vdf]
@@ -820,7 +906,18 @@ struct Tc2Args {
     int region;  // bytes per VDF tile in an item slot: A hi, A lo, f(c1) (FP32)
 };
 
-template <int VB, int P>
+// MODE 0: Q(f,f), a CTA owns output cells D and an item (block c1, c2) reads
+//         F16 tiles of cells c2 + D and the FP32 side tile of cells c1 + D;
+//         per row acc[p] += f(c1+D, l1) G[(l1, p)].
+// MODE 1: the adjoint g = J(f)^T v (block form of the VJP), a CTA owns
+//         target cells T; an item is one of the two scatters of a block:
+//           W1 (pass 1, to the c1 side): G = f(c2+D) W1, D = T - c1,
+//           W2 (pass 2, to the c2 side): G = f(c1+D) W2, D = T - c2,
+//         its c1/c2 fields hold ccell + (side cell - T) and ccell + (F16
+//         cell - T); the side tile is c = 2v/w at cells D, the records'
+//         columns are p-major (n = p*P + l) and per row
+//         acc[l] += c(D, p) G[(p, l)], the forward's pattern.
+template <int VB, int P, int MODE>
 __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
 {
     constexpr int NDG = TC_ROWS / VB;
@@ -865,6 +962,19 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    if (warp >= 2) {
+        // zero all 512 columns once (warps 2-5 the first 256, 6-9 the rest, each
+        // its lane quarter): an item's last column group may be narrower than
+        // the 64-column loads of the epilogue, whose extra columns then hold
+        // zeros or finite values of earlier jobs, times a zero factor
+        const float z[16] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const uint32_t tq = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(((warp - 2) >> 2) * 256);
+#pragma unroll 1
+        for (int cz = 0; cz < 256; cz += 16) tmem_st16(tq + (uint32_t)cz, z);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
 
     if (warp == 0) {
         // ---------------- producer ----------------
@@ -904,11 +1014,17 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                     mbar_arrive(&s_full[s]);
                 }
                 q++;
-                for (int g = 0; g < NG; g++, gw++) {
+                // MODE 0: the block's compacted record (chunk0 = its first
+                // group); MODE 1: W1 or W2 of block chunk0 & 0x3fffffff
+                const int ngb = MODE == 0 ? t2_item_groups<P>(e.nch) : NG;
+                const unsigned char *wrec =
+                    MODE == 0 ? a.W + (size_t)e.chunk0 * T2_GREC
+                              : ((e.chunk0 >> 30) ? a.W2 : a.W) + (size_t)(e.chunk0 & 0x3fffffff) * NG * T2_GREC;
+                for (int g = 0; g < ngb; g++, gw++) {
                     const int st = gw % T2_NSTW;
                     if (!mbar_wait(&w_empty[st], ((gw / T2_NSTW) & 1) ^ 1, a.err)) { ok = false; break; }
                     mbar_arrive_expect_tx(&w_full[st], T2_GREC);
-                    bulk_g2s(wring + st * T2_GREC, a.W + ((size_t)e.chunk0 * NG + g) * T2_GREC, T2_GREC, &w_full[st]);
+                    bulk_g2s(wring + st * T2_GREC, wrec + (size_t)g * T2_GREC, T2_GREC, &w_full[st]);
                 }
             }
             if (!ok) {  // let the copies already issued land
@@ -921,23 +1037,25 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            // FP32 accumulator, fp16 A and B, both K-major, M = 128, N = 128
-            // the last group holds P*P - 256 (NG-1) columns: its MMAs use
-            // N rounded up to 16, not 256
-            constexpr int NLAST = ((P * P - (NG - 1) * T2_N) + 15) / 16 * 16;
+            // FP32 accumulator, fp16 A and B, both K-major, M = 128, N = 256;
+            // an item's last group holds ncol - 256 (ngb-1) columns: its MMAs
+            // use N rounded up to 16
             const uint32_t idesc = (1u << 4) | ((uint32_t)(T2_N >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
-            const uint32_t idesc_last = (1u << 4) | ((uint32_t)(NLAST >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             int q = 0, gw = 0, J = 0;
             bool ok = true;
             for (int it = i0; it < i1 && ok; it++) {
                 const int s = q & 1;
+                const int ncol = MODE == 0 ? __popc((unsigned)a.items[it].nch & 0x7ffffffu) * P : P * P;
+                const int ngb = (ncol + T2_N - 1) / T2_N;
+                const int nlast = ((ncol - (ngb - 1) * T2_N) + 15) / 16 * 16;
+                const uint32_t idesc_last = (1u << 4) | ((uint32_t)(nlast >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
                 if (!mbar_wait(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
-                for (int g = 0; g < NG && ok; g++, gw++) {
+                for (int g = 0; g < ngb && ok; g++, gw++) {
                     const int st = gw % T2_NSTW;
                     if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err)) { ok = false; break; }
                     const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
                     const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
-                    const uint32_t id = g == NG - 1 ? idesc_last : idesc;
+                    const uint32_t id = g == ngb - 1 ? idesc_last : idesc;
                     for (int j = 0; j < nb2; j++, J++) {
                         const int cs = J & 1;
                         if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
@@ -974,35 +1092,65 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         float S[P], Cc[P];
 #pragma unroll
         for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
-        int q = 0;
+        int q = 0, gq = 0;  // items and column groups consumed so far
         bool ok = true;
         for (int it = i0; it < i1 && ok; it++) {
-            const bool valid = (a.items[it].nch >> (16 + d)) & 1;
+            const int nch = a.items[it].nch;
+            const bool valid = (nch >> (27 + d)) & 1;
+            const unsigned msk = (unsigned)nch & 0x7ffffffu;
+            const int nl = MODE == 0 ? __popc(msk) : P, ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
             const int s = q & 1;
             if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
             const float *f1s =
                 reinterpret_cast<const float *>(slots + (size_t)(2 * s + j) * a.region + 2 * T2_ATILE) + d * P * VB + v;
-            float f1[P], acc[P];
+            // side factor of the item's rows: f(c1 + D, l1) for the j-th node
+            // l1 of the mask (MODE 0, columns n = j*P + p; 0 for j past the
+            // mask's nodes) or c(D, p) (MODE 1, columns n = p*P + l); either
+            // way acc[n % P] += side[n / P] * G[n]
+            // (MODE 0 loads each factor at its first column: all 27 live at
+            // once, with the mask lookups, would spill)
+            float f1[P], acc[P], fcur = 0.f;
 #pragma unroll
-            for (int l = 0; l < P; l++) { f1[l] = f1s[l * VB]; acc[l] = 0.f; }
+            for (int l = 0; l < P; l++) {
+                if (MODE == 1) f1[l] = f1s[l * VB];
+                acc[l] = 0.f;
+            }
 #pragma unroll
             for (int g = 0; g < NG; g++) {
-                const int J = (q * NG + g) * nb2 + j, cs = J & 1;
+                if (g >= ngb) break;
+                const int J = (gq + g) * nb2 + j, cs = J & 1;
                 if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, a.err)) { ok = false; break; }
                 tc_fence_after();
                 // two 32-column loads per wait: the load latency is paid
                 // four times per 256-column group
 #pragma unroll
                 for (int hh = 0; hh < T2_N / 64; hh++) {
-                    if (g * T2_N + 64 * hh >= P * P) break;
+                    if (g * T2_N + 64 * hh >= P * P || g * T2_N + 64 * hh >= ncol) break;
                     uint32_t G[64];
                     tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh), G);
-                    if (g * T2_N + 64 * hh + 32 < P * P) tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh + 32), G + 32);
+                    if (g * T2_N + 64 * hh + 32 < P * P) {
+                        if (g * T2_N + 64 * hh + 32 < ncol) {
+                            tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh + 32), G + 32);
+                        } else {
+#pragma unroll
+                            for (int i = 32; i < 64; i++) G[i] = 0u;
+                        }
+                    }
                     tmem_wait_ld();
 #pragma unroll
                     for (int i = 0; i < 64; i++) {
                         const int n = g * T2_N + 64 * hh + i;
-                        if (n < P * P) acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
+                        if (n < P * P) {
+                            if constexpr (MODE == 0) {
+                                if (n % P == 0 || i == 0) {
+                                    const int jj = n / P;
+                                    fcur = jj < nl ? f1s[__fns(msk, 0u, jj + 1) * VB] : 0.f;
+                                }
+                                acc[n % P] = fmaf(fcur, __uint_as_float(G[i]), acc[n % P]);
+                            } else {
+                                acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
+                            }
+                        }
                     }
                 }
                 tc_fence_before();
@@ -1010,6 +1158,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                 if (lane == 0) mbar_arrive(&c_empty[cs]);
             }
             if (!ok) break;
+            gq += ngb;
             __syncwarp();
             if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
             if (valid) {
@@ -1025,7 +1174,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         if (ok) {
             const int D = D0 + d, vdf = (bt0 + j) * VB + v;
             if (D < a.Nc && vdf < a.nvdf) {
-                const double sc = a.inv_scale[vdf];
+                const double sc = MODE == 0 ? a.inv_scale[vdf] : 1.0;  // the adjoint scales in k_tc_vjp_final
 #pragma unroll
                 for (int p = 0; p < P; p++) {
                     double *dst = a.qacc + ((size_t)D * P + p) * a.NV + vdf;
@@ -1041,26 +1190,49 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }
 
+// Block records of the collision operator, compacted to the nodes l1 each
+// block uses: a mask per block (device pass over the pairs), the blocks'
+// group offsets on the host, then the records.
 static int tc2_prepare(Ctx *c)
 {
     Layout &L = c->lay;
     if (L.tc2_W) return DGV_OK;
     const Grid &g = c->grid;
-    const int NG = t2_groups(g.P);
     int rc = tc_value_scale(c, &L.tc2_vscale);
     if (rc) return rc;
-    const size_t rec = (size_t)NG * T2_GREC;
-    cudaError_t e = cudaMalloc(&L.tc2_W, (size_t)std::max<long long>(1, L.nblocks) * rec);
-    if (e != cudaSuccess) {
+    const long long nb = L.nblocks;
+    L.tc2_mask.assign((size_t)nb, 0u);
+    L.tc2_goff.assign((size_t)nb + 1, 0);
+    unsigned *d_mask = nullptr;
+    long long *d_goff = nullptr;
+    DGV_CUDA(c, cudaMalloc(&d_mask, sizeof(unsigned) * std::max<long long>(1, nb)));
+    if (nb) {
+        k_tc2_mask<<<(unsigned)nb, 128, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.Nc, g.ccell, d_mask);
+        DGV_CUDA(c, cudaGetLastError());
+        DGV_CUDA(c, cudaMemcpyAsync(L.tc2_mask.data(), d_mask, sizeof(unsigned) * nb, cudaMemcpyDeviceToHost, c->stream));
+        DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    for (long long b = 0; b < nb; b++)
+        L.tc2_goff[b + 1] = L.tc2_goff[b] + (__builtin_popcount(L.tc2_mask[b]) * g.P + T2_N - 1) / T2_N;
+    const size_t bytes = (size_t)std::max<long long>(1, L.tc2_goff[nb]) * T2_GREC;
+    cudaError_t e = cudaMalloc(&L.tc2_W, bytes);
+    if (e != cudaSuccess || cudaMalloc(&d_goff, sizeof(long long) * (nb + 1)) != cudaSuccess) {
         cudaGetLastError();
+        if (L.tc2_W) cudaFree(L.tc2_W);
         L.tc2_W = nullptr;
+        cudaFree(d_mask);
         return set_err(c, DGV_ENOMEM, "tensor-core block form: no room for the block records");
     }
-    if (L.nblocks)
-        k_tc2_build<<<(unsigned)L.nblocks, 256, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.P, g.Nc,
-                                                                 g.ccell, (float)L.tc2_vscale,
-                                                                 (unsigned char *)L.tc2_W);
+    DGV_CUDA(c, cudaMemcpyAsync(d_goff, L.tc2_goff.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice,
+                                c->stream));
+    if (nb)
+        k_tc2_build<<<(unsigned)nb, 256, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.P, g.Nc, g.ccell,
+                                                          (float)L.tc2_vscale, (unsigned char *)L.tc2_W, 0, d_mask,
+                                                          d_goff);
     DGV_CUDA(c, cudaGetLastError());
+    DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(d_mask);
+    cudaFree(d_goff);
     return DGV_OK;
 }
 
@@ -1074,32 +1246,40 @@ static void tc2_sets(Ctx *c)
         if (it->first >= 256) {
             for (void *p : it->second) cudaFree(p);
             L.tc_list_work.erase(it->first);
+            L.tc_list_items.erase(it->first);
             it = L.tc_lists.erase(it);
         } else {
             ++it;
         }
     }
-    const long long rec = (long long)t2_groups(c->grid.P) * T2_GREC;
+    // about tc_set_mb MB of the collision operator's (compacted) records per set
     L.tc2_sets.clear();
     L.tc2_sets.push_back(0);
-    const long long per_set = std::max<long long>(1, ((long long)c->tc_set_mb << 20) / rec);
-    for (long long b = per_set; b < L.nblocks; b += per_set) L.tc2_sets.push_back((int)b);
+    const long long per_set = std::max<long long>(1, ((long long)c->tc_set_mb << 20) / T2_GREC);
+    long long acc = 0;
+    for (long long b = 0; b < L.nblocks; b++) {
+        acc += L.tc2_goff[b + 1] - L.tc2_goff[b];
+        if (acc >= per_set && b + 1 < L.nblocks) {
+            L.tc2_sets.push_back((int)(b + 1));
+            acc = 0;
+        }
+    }
     if (L.tc2_sets.back() != (int)L.nblocks) L.tc2_sets.push_back((int)L.nblocks);
     L.tc2_set_mb = c->tc_set_mb;
 }
 
-template <int VB, int P>
+template <int VB, int P, int MODE = 0>
 static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng)
 {
     const size_t smem = (size_t)T2_NSTW * T2_GREC + 4 * (size_t)a.region + (2 * T2_NSTW + 13) * sizeof(uint64_t) + 16;
-    DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc2<VB, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+    DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc2<VB, P, MODE>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const Layout &L = c->lay;
     KTimer kt(c);
     for (size_t s = 0; s + 1 < L.tc2_sets.size(); s++) {
         a.item_start = tl.item_start + s * (ng + 1);
         a.tile_of = tl.tile_of + s * ng;
-        k_collide_tc2<VB, P><<<(unsigned)(a.nbp * ng), T2_THREADS, smem, c->stream>>>(a);
+        k_collide_tc2<VB, P, MODE><<<(unsigned)(a.nbp * ng), T2_THREADS, smem, c->stream>>>(a);
         DGV_CUDA(c, cudaGetLastError());
     }
     kt.stop((long long)L.tc2_sets.size() - 1);
@@ -1107,13 +1287,13 @@ static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng)
     return DGV_OK;
 }
 
-template <int P>
+template <int P, int MODE = 0>
 static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, int VB)
 {
     switch (VB) {
-    case 128: return launch_tc2<128, P>(c, a, tl, ng);
-    case 64: return launch_tc2<64, P>(c, a, tl, ng);
-    default: return launch_tc2<32, P>(c, a, tl, ng);
+    case 128: return launch_tc2<128, P, MODE>(c, a, tl, ng);
+    case 64: return launch_tc2<64, P, MODE>(c, a, tl, ng);
+    default: return launch_tc2<32, P, MODE>(c, a, tl, ng);
     }
 }
 
@@ -1137,21 +1317,20 @@ static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, 
     if (rc) return rc;
     TcLists tl;
     {
-        std::vector<int> first(L.nblocks), count(L.nblocks, 1);
-        std::iota(first.begin(), first.end(), 0);
-        rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl);
+        std::vector<int> first, count;
+        rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl, 1);
         if (rc) return rc;
     }
     float *F = reinterpret_cast<float *>(c->d_tcF);
     unsigned char *F16 = reinterpret_cast<unsigned char *>(c->d_tcF) + fbytes;
     double *inv = reinterpret_cast<double *>(F16 + f16bytes);
-    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc2_vscale, F, inv, g.Nc, g.P, VB);
+    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc2_vscale, F, inv, g.Nc, g.P, VB, 2);
     DGV_CUDA(c, cudaGetLastError());
     k_tc2_f16<<<1184, 256, 0, c->stream>>>(F, F16, nbt, g.Nc, g.P, VB);
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
     Tc2Args a;
-    a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.items = tl.items;
+    a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.W2 = nullptr; a.items = tl.items;
     a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
     a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
     a.tpc = c->tc_tiles_per_cta;
@@ -1164,6 +1343,145 @@ static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, 
     DGV_CUDA(c, cudaGetLastError());
     count_launches(c, 3);  // k_tc_fprep, k_tc2_f16, k_tc_final
     if (c->project) return project_device(c, d_q, nvdf);
+    return DGV_OK;
+}
+
+// ----------------------------------------------------------------------------
+// Block-form adjoint (VJP): g = J(f)^T v for a batch, on the tensor cores.
+// With c_i = 2 v_i / w_i and Q_i = (2/w_i) sum_j A_j f(a_j) f(b_j), the
+// adjoint of collision_mod.f90:213-216 scatters c_i A_j f(b_j) to a_j and
+// c_i A_j f(a_j) to b_j.  Per block and output cell D these are
+//   g(c1+D, l1) += sum_p c(D,p) G1[(D,b), (p,l1)], G1 = F2 W1 (the forward's
+//                  product, columns reordered p-major),
+//   g(c2+D, l2) += sum_p c(D,p) G2[(D,b), (p,l2)], G2 = F1 W2 (the block's
+//                  values with the two nodes' roles swapped),
+// so the kernel is the forward's with target-cell ownership (MODE 1).
+
+// per-VDF power-of-two scale of c = 2 v / w (max |c| -> [32, 64)) and the
+// scaled FP32 copy in the layout of F; inv_c[v] = the inverse scale
+__global__ void k_tc_cprep(const double *vv, const double *w, long long N, int nvdf, float *C, double *inv_c, int Nc,
+                           int P, int VB)
+{
+    const int v = blockIdx.x;
+    __shared__ double red[32];
+    double m = 0.0;
+    if (v < nvdf)
+        for (long long i = threadIdx.x; i < N; i += blockDim.x) m = fmax(m, fabs(2.0 * vv[(size_t)v * N + i] / w[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) red[0] = m;
+    }
+    __syncthreads();
+    m = red[0];
+    int e = 0;
+    if (m > 0.0) {
+        frexp(m, &e);
+        e = 6 - e;
+    }
+    const double sc = ldexp(1.0, e);
+    if (threadIdx.x == 0) inv_c[v] = ldexp(1.0, -e);
+    const int bt = v / VB, lb = v % VB;
+    for (long long i = threadIdx.x; i < N; i += blockDim.x) {
+        const int cell = (int)(i / P), l = (int)(i - (long long)cell * P);
+        const double x = v < nvdf ? 2.0 * vv[(size_t)v * N + i] / w[i] * sc : 0.0;
+        C[(((size_t)bt * Nc + cell) * P + l) * VB + lb] = (float)x;
+    }
+}
+
+// g[v][i] = gacc[i*NV + v] * inv_f[v] * inv_c[v]
+__global__ void k_tc_vjp_final(const double *gacc, const double *inv_f, const double *inv_c, double *g, long long N,
+                               int nvdf, int NV)
+{
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nvdf * N) return;
+    const int v = (int)(idx % nvdf);
+    const long long i = idx / nvdf;
+    g[(size_t)v * N + i] = gacc[i * NV + v] * inv_f[v] * inv_c[v];
+}
+
+// the adjoint's block records W1 and W2 (arrangements 1 and 2 of
+// k_tc2_build), built on the first adjoint call with the value scale of W
+static int tc2_prepare_adjoint(Ctx *c)
+{
+    Layout &L = c->lay;
+    if (L.tc2_Wv[0] && L.tc2_Wv[1]) return DGV_OK;
+    const Grid &g = c->grid;
+    const size_t rec = (size_t)t2_groups(g.P) * T2_GREC;
+    for (int k = 0; k < 2; k++) {
+        if (L.tc2_Wv[k]) continue;
+        cudaError_t e = cudaMalloc(&L.tc2_Wv[k], (size_t)std::max<long long>(1, L.nblocks) * rec);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            L.tc2_Wv[k] = nullptr;
+            return set_err(c, DGV_ENOMEM, "tensor-core adjoint: no room for its block records");
+        }
+        if (L.nblocks)
+            k_tc2_build<<<(unsigned)L.nblocks, 256, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.P,
+                                                                     g.Nc, g.ccell, (float)L.tc2_vscale,
+                                                                     (unsigned char *)L.tc2_Wv[k], k + 1, nullptr,
+                                                                     nullptr);
+        DGV_CUDA(c, cudaGetLastError());
+    }
+    return DGV_OK;
+}
+
+int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int nvdf)
+{
+    const Grid &g = c->grid;
+    Layout &L = c->lay;
+    if (!L.blk) return set_err(c, DGV_ESTATE, "vjp: no A-arrays loaded");
+    if (g.P != 27 && g.P != 8)
+        return set_err(c, DGV_EUNSUP, "tensor-core adjoint: grids of 8 or 27 nodes per cell");
+    if (nvdf < 1) return set_err(c, DGV_EINVAL, "vjp: batch must hold at least one VDF");
+    int rc = tc2_prepare(c);
+    if (rc) return rc;
+    if ((rc = tc2_prepare_adjoint(c))) return rc;
+    tc2_sets(c);
+    if ((rc = ensure_errflag(c))) return rc;
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), NDG = TC_ROWS / VB;
+    const int nbt = (nvdf + VB - 1) / VB, NV = nbt * VB, ng = (g.Nc + NDG - 1) / NDG;
+    const size_t fbytes = (size_t)nbt * g.Nc * g.P * VB * sizeof(float);
+    const size_t f16bytes = (size_t)nbt * 2 * g.Nc * VB * T2_K * 2;
+    const size_t gbytes = (size_t)g.N * NV * sizeof(double);
+    rc = ensure_buffer(c, &c->d_tcF, &c->tcF_bytes, 2 * fbytes + f16bytes + 2 * NV * sizeof(double));
+    if (rc) return rc;
+    rc = ensure_buffer(c, &c->d_tcQ, &c->tcQ_bytes, gbytes);
+    if (rc) return rc;
+    TcLists tl;
+    {
+        std::vector<int> first, count;
+        rc = tc_work_lists(c, NDG, 512 + NDG, L.tc2_sets, first, count, &tl, 2);
+        if (rc) return rc;
+    }
+    float *F = reinterpret_cast<float *>(c->d_tcF);
+    unsigned char *F16 = reinterpret_cast<unsigned char *>(c->d_tcF) + fbytes;
+    float *Cf = reinterpret_cast<float *>(F16 + f16bytes);
+    double *inv_f = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(Cf) + fbytes);
+    double *inv_c = inv_f + NV;
+    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc2_vscale, F, inv_f, g.Nc, g.P, VB, 1);
+    DGV_CUDA(c, cudaGetLastError());
+    k_tc2_f16<<<1184, 256, 0, c->stream>>>(F, F16, nbt, g.Nc, g.P, VB);
+    DGV_CUDA(c, cudaGetLastError());
+    k_tc_cprep<<<NV, 256, 0, c->stream>>>(d_v, c->d_nwt, g.N, nvdf, Cf, inv_c, g.Nc, g.P, VB);
+    DGV_CUDA(c, cudaGetLastError());
+    DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, gbytes, c->stream));
+    Tc2Args a;
+    a.F = Cf; a.F16 = F16; a.W = (const unsigned char *)L.tc2_Wv[0]; a.W2 = (const unsigned char *)L.tc2_Wv[1];
+    a.items = tl.items; a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = nullptr;
+    a.err = c->d_err; a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
+    a.tpc = c->tc_tiles_per_cta;
+    a.nbp = (nbt + a.tpc - 1) / a.tpc;
+    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + 1023) / 1024 * 1024;
+    rc = g.P == 27 ? launch_tc2_vb<27, 1>(c, a, tl, ng, VB) : launch_tc2_vb<8, 1>(c, a, tl, ng, VB);
+    if (rc) return rc;
+    const long long tot = (long long)nvdf * g.N;
+    k_tc_vjp_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, inv_f, inv_c, d_g, g.N, nvdf, NV);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 4);  // k_tc_fprep, k_tc2_f16, k_tc_cprep, k_tc_vjp_final
     return DGV_OK;
 }
 
@@ -1208,20 +1526,19 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
     }
     if (block) {
         tc2_sets(c);
-        std::vector<int> first(L.nblocks), count(L.nblocks, 1);
-        std::iota(first.begin(), first.end(), 0);
-        if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl))) return rc;
-        const long long w = L.tc_list_work[256 + NDG];
+        std::vector<int> first, count;
+        if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl, 1))) return rc;
+        // per item and VDF tile: 2 K steps x 3 split products over its issued columns
+        const long long cols = L.tc_list_work[256 + NDG];
         *launches = (long long)L.tc2_sets.size() - 1;
-        *items = w * nbt;
-        const int ng2 = t2_groups(g.P), nlast = ((g.P * g.P - (ng2 - 1) * T2_N) + 15) / 16 * 16;
-        *flop = (double)w * nbt * ((ng2 - 1) * T2_N + nlast) * 6.0 * 2.0 * TC_ROWS * 16;
+        *items = L.tc_list_items[256 + NDG] * nbt;
+        *flop = (double)cols * nbt * 6.0 * 2.0 * TC_ROWS * 16;
     } else {
         if ((rc = tc_prepare(c))) return rc;
         if ((rc = tc_lists(c, NDG, &tl))) return rc;
         const long long w = L.tc_list_work[NDG];
         *launches = (long long)L.tc_sets.size() - 1;
-        *items = w * nbt;
+        *items = w * nbt;  // chunk x row tile
         *flop = (double)w * nbt * 4.0 * 2.0 * TC_ROWS * 16 * (64 + 32);
     }
     return DGV_OK;
@@ -1260,7 +1577,7 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
     if (rc) return rc;
     float *F = reinterpret_cast<float *>(c->d_tcF);
     double *inv = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_tcF) + fbytes);
-    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc_vscale, F, inv, g.Nc, g.P, VB);
+    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc_vscale, F, inv, g.Nc, g.P, VB, 2);
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
     TcArgs a;

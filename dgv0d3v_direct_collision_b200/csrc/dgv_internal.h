@@ -74,13 +74,20 @@ struct Layout {
     // block form (built on first use): per block the dense split-fp16 tiles
     // W[l2][(l1, p)] of its values, the value scale, and the block sets
     void *tc2_W = nullptr;  // device
+    void *tc2_Wv[2] = {nullptr, nullptr};  // device: the adjoint's records (built on first use)
     double tc2_vscale = 1.0;
     std::vector<int> tc2_sets;
     int tc2_set_mb = 0;  // record megabytes per set the sets were built for
     // device work lists {items, item starts, tile order}, keyed by cells per
     // tile (chunk form) or 256 + cells per tile (block form)
     std::map<int, std::vector<void *>> tc_lists;
-    std::map<int, long long> tc_list_work;  // per key: sum of the items' counts
+    std::map<int, long long> tc_list_work;   // per key: sum of the items' work (chunk records / issued columns)
+    std::map<int, long long> tc_list_items;  // per key: number of items
+    // block form: per block the mask of its nodes l1 (bit l1 set if the
+    // block has a pair with it) and the first record group of the block's
+    // compacted records (nblocks + 1 entries, host)
+    std::vector<uint32_t> tc2_mask;
+    std::vector<long long> tc2_goff;
 };
 void free_layout(Layout &L);
 
@@ -161,6 +168,12 @@ int set_err(Ctx *c, int code, const std::string &msg);
     } while (0)
 
 int ensure_buffer(Ctx *c, double **p, size_t *have, size_t need_bytes);
+// *dev = true for memory of c's device (or managed), false for host memory;
+// DGV_EINVAL for device memory of another GPU
+int classify_ptr(Ctx *c, const void *p, bool *dev);
+// loads the no-allocation path's static work array on c's device (the
+// runtime loads modules lazily), so that it is reserved from context creation
+void noalloc_prepare(Ctx *c);
 void release_graphs(const Ctx *c);
 int ensure_errflag(Ctx *c);
 int check_errflag(Ctx *c);
@@ -181,6 +194,7 @@ int collide_tc_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double s
 int collide_cells_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, int cell0, int cell1);
 int jvp_device(Ctx *c, const double *d_f, const double *d_df, double *d_q, int precision);
 int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int precision);
+int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int nvdf);
 int moments_device(Ctx *c, const double *d_f, int nvdf, double *h_out);
 int project_device(Ctx *c, double *d_q, int nvdf);
 int maxwellian_device(Ctx *c, double T, double u0, double v0, double w0, double n, double *d_f);

@@ -18,7 +18,6 @@
 namespace dgv {
 
 int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, double scale);
-bool is_device_pointer(const void *p);
 
 namespace {
 
@@ -119,8 +118,9 @@ extern "C" int dgv_collide_group(int32_t n, dgv_ctx *const *ctxs, const int32_t 
         c->err.clear();
         if (c->device != c0->device) return set_err(c0, DGV_EINVAL, "collide_group: contexts on different devices");
         if (nb[i] < 1 || !f[i] || !q[i]) return set_err(c0, DGV_EINVAL, "collide_group: need nb >= 1 and arrays");
-        if (!is_device_pointer(f[i]) || !is_device_pointer(q[i]))
-            return set_err(c0, DGV_EINVAL, "collide_group: f and q must be device pointers");
+        bool fdev = false, qdev = false;
+        if (classify_ptr(c, f[i], &fdev) || classify_ptr(c, q[i], &qdev) || !fdev || !qdev)
+            return set_err(c0, DGV_EINVAL, "collide_group: f and q must be device pointers of the members' device");
         if (!c->lay.blk) return set_err(c0, DGV_ESTATE, "collide_group: a member has no A-arrays loaded");
         Member mb;
         std::memset(&mb, 0, sizeof(mb));

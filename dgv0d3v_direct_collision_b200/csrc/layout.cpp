@@ -29,6 +29,8 @@ void free_layout(Layout &L)
     if (L.tc_V) cudaFree(L.tc_V);
     if (L.tc_chunk_start) cudaFree(L.tc_chunk_start);
     if (L.tc2_W) cudaFree(L.tc2_W);
+    for (void *w : L.tc2_Wv)
+        if (w) cudaFree(w);
     for (auto &kv : L.tc_lists)
         for (void *p : kv.second) cudaFree(p);
     L = Layout();

@@ -12,15 +12,17 @@
 //
 // The work buffer of the FP64 collision kernel (the per-chunk partial sums
 // that the fixed-order reduction adds up) lives instead in the file-scope
-// array below, whose size is fixed when the library is loaded: every GPU that
-// loads libdgv_b200.so holds these 32 MiB until the process exits.  In host
-// code the array's name is only a stand-in for the device symbol, so the host
-// asks the runtime for its device address (cudaGetSymbolAddress) once per
-// device, with that device current, and passes that pointer to the kernels.
+// array below, whose size is fixed at build time: 32 MiB on every GPU on which
+// a context is created.  The CUDA runtime loads a library's device code and
+// data lazily, so dgv_ctx_create loads this array on its device at once (a
+// pool allocator set up after the context cannot take its room); it stays
+// until the process exits.  In host code the array's name is only a stand-in
+// for the device symbol, so every call asks the runtime for its device
+// address (cudaGetSymbolAddress) with the context's device current and passes
+// that pointer to the kernels.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 
 #include "dgv_internal.h"
@@ -31,26 +33,19 @@ namespace dgv {
 constexpr long long NOALLOC_SCRATCH_DOUBLES = 1LL << 22;
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-static std::mutex g_noalloc_mu;
-static double *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // device address per device ordinal
-
-// Device address of g_noalloc_scratch on `device` (must be current).  Looked
-// up on the first call per device and cached.
+// Device address of g_noalloc_scratch on c's device (current), looked up on
+// every call: cheap once the module is loaded, and still right after the host
+// program reset the device (which unloads it).
 static int noalloc_scratch(Ctx *c, double **out)
 {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (c->device < 0 || c->device >= NOALLOC_MAX_DEVICES)
-        return set_err(c, DGV_EUNSUP, "no-alloc scratch: device ordinal above 63");
-    if (!g_noalloc_addr[c->device]) {
-        double *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return set_err(c, DGV_ECUDA, std::string("no-alloc scratch: cudaGetSymbolAddress failed: ") +
-                                             cudaGetErrorString(e));
-        g_noalloc_addr[c->device] = p;
+    double *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return set_err(c, DGV_ECUDA, std::string("no-alloc scratch: cudaGetSymbolAddress failed: ") +
+                                         cudaGetErrorString(e));
     }
-    *out = g_noalloc_addr[c->device];
+    *out = p;
     return DGV_OK;
 }
 
@@ -135,14 +130,31 @@ __global__ void k_reduce_noalloc(const double *partial, const double *w, double 
 
 typedef void (*NoAllocFn)(NoAllocArgs);
 
-static bool on_device(const void *p)
+static NoAllocFn noalloc_kernel(int P)
 {
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
+    switch (P) {
+    case 1: return k_collide_f64_noalloc<1>;
+    case 8: return k_collide_f64_noalloc<8>;
+    case 27: return k_collide_f64_noalloc<27>;
+    default: return nullptr;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// Called by dgv_ctx_create with the device current: loads the module holding
+// the static array (reserving its 32 MiB now rather than at the first call)
+// and raises the kernel's shared-memory limit.  Failures are not fatal to the
+// context; the first no-alloc call reports them.
+void noalloc_prepare(Ctx *c)
+{
+    double *p = nullptr;
+    if (noalloc_scratch(c, &p)) c->err.clear();
+    NoAllocFn fn = noalloc_kernel(c->grid.P);
+    const size_t smem = (size_t)c->grid.N * sizeof(double);
+    int maxsm = 0;
+    if (fn && cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) == cudaSuccess &&
+        smem <= (size_t)maxsm)
+        cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaGetLastError();
 }
 
 static int collide_noalloc(Ctx *c, const double *f, double *q, int nb, cudaStream_t st)
@@ -151,15 +163,14 @@ static int collide_noalloc(Ctx *c, const double *f, double *q, int nb, cudaStrea
     const Layout &L = c->lay;
     if (!L.blk) return set_err(c, DGV_ESTATE, "collide_noalloc: no A-arrays loaded");
     if (nb < 1 || !f || !q) return set_err(c, DGV_EINVAL, "collide_noalloc: need nb >= 1 and non-NULL arrays");
-    if (!on_device(f) || !on_device(q))
-        return set_err(c, DGV_EINVAL, "collide_noalloc: f and q must be device (or managed) memory");
-    NoAllocFn fn = nullptr;
-    switch (g.P) {
-    case 1: fn = k_collide_f64_noalloc<1>; break;
-    case 8: fn = k_collide_f64_noalloc<8>; break;
-    case 27: fn = k_collide_f64_noalloc<27>; break;
-    default: return set_err(c, DGV_EUNSUP, "collide_noalloc: 1, 8 or 27 nodes per cell");
-    }
+    bool fdev = false, qdev = false;
+    int rc = classify_ptr(c, f, &fdev);
+    if (rc) return rc;
+    if ((rc = classify_ptr(c, q, &qdev))) return rc;
+    if (!fdev || !qdev)
+        return set_err(c, DGV_EINVAL, "collide_noalloc: f and q must be device (or managed) memory of the context's device");
+    NoAllocFn fn = noalloc_kernel(g.P);
+    if (!fn) return set_err(c, DGV_EUNSUP, "collide_noalloc: 1, 8 or 27 nodes per cell");
     const long long per_chunk = (long long)nb * g.N;  // doubles of partials per chunk
     if (per_chunk > NOALLOC_SCRATCH_DOUBLES)
         return set_err(c, DGV_EINVAL,
@@ -177,7 +188,7 @@ static int collide_noalloc(Ctx *c, const double *f, double *q, int nb, cudaStrea
     long long fit = NOALLOC_SCRATCH_DOUBLES / per_chunk;
     int nchunks = (int)std::max<long long>(1, std::min<long long>({want, fit, std::max<long long>(1, L.nblocks), 65535LL}));
     double *scratch = nullptr;
-    int rc = noalloc_scratch(c, &scratch);
+    rc = noalloc_scratch(c, &scratch);
     if (rc) return rc;
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     NoAllocArgs a;

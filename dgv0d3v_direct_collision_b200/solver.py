@@ -267,10 +267,16 @@ class DGVSolver:
     def jvp(self, f, df, out=None):
         return self.EvalCollisionPeriodicMixedTermsA_DGV(df, f, out)
 
-    def vjp(self, f, v, out=None):
+    def vjp(self, f, v, out=None, precision="f64"):
+        """g = J(f)^T v for one VDF or a batch [nb, N] (dgv_vjp_batched);
+        precision "f64" (FP64 kernel per VDF) or "tc" (block form on the
+        tensor cores, all VDFs in one pass)."""
         _check_f64(f); _check_f64(v)
+        if tuple(f.shape) != tuple(v.shape) or f.shape[-1] != self.N:
+            raise ValueError("vjp: f and v must have the same shape [..., N]")
         out = self._like(f) if out is None else out
-        self._check(self._lib.dgv_vjp(self._h, _ptr(f), _ptr(v), _ptr(out), DGV_PREC_F64))
+        nb = int(np.prod(f.shape)) // self.N
+        self._check(self._lib.dgv_vjp_batched(self._h, nb, _ptr(f), _ptr(v), _ptr(out), self._prec(precision)))
         return out
 
     def PrepareFMA_DGV(self, fm):

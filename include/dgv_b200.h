@@ -220,14 +220,18 @@ int dgv_collide_cells(dgv_ctx *ctx, int32_t nb, const double *f, double *q, int3
  * driver that gives all free memory to its own pool allocator at start-up, or
  * a process held to a fixed memory budget on a shared GPU, where a cudaMalloc
  * in the time loop would fail or stall the device.  This call allocates
- * nothing: f and q are caller-owned device arrays [nb][N], and the kernel's
- * partial sums go to a static 32 MiB device array that every GPU loading the
- * library holds until the process exits.  Limit: nb*N <= 4194304 (2^22)
- * doubles, else DGV_EINVAL.  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  All calls
- * share the array and leave their partial sums in it: calls that overlap on
- * the GPU (other streams or host threads) race, so serialise them.  No
- * conservation projection.  stream NULL = the context's stream. */
+ * nothing: f and q are caller-owned device arrays [nb][N] of the context's
+ * device, and the kernel's partial sums go to a static 32 MiB device array.
+ * The CUDA runtime loads device data lazily, so dgv_ctx_create loads that
+ * array on its device: create the context before a pool allocator takes the
+ * free memory; the 32 MiB stay reserved until the process exits.  Each call
+ * looks up the array's device address (no allocation); after the host program
+ * resets the device, make the next call outside any stream capture (the
+ * lookup reloads the array).  Limit: nb*N <= 4194304 (2^22) doubles, else
+ * DGV_EINVAL.  All calls share the array and leave their partial sums in it:
+ * calls that overlap on the GPU (other streams or host threads) race, so
+ * serialise them.  No conservation projection.  stream NULL = the context's
+ * stream. */
 int dgv_collide_f64_noalloc(dgv_ctx *ctx, const double *f, double *q, int32_t nb, void *stream);
 
 /* -- time integration ------------------------------------------------------ */
@@ -278,12 +282,25 @@ int dgv_project(dgv_ctx *ctx, double *q, int32_t nb);
 
 /* -- derivatives ----------------------------------------------------------- */
 /* q = 2/w * sum A (f(xi) df(xi1) + df(xi) f(xi1)): the Jacobian-vector product
- * of Q at f (EvalCollisionPeriodicMixedTermsA_DGV, collision_mod.f90:244-332). */
+ * of Q at f (EvalCollisionPeriodicMixedTermsA_DGV, collision_mod.f90:244-332).
+ * FP64 only: other precisions give DGV_EUNSUP (as dgv_apply_linear). */
 int dgv_jvp(dgv_ctx *ctx, const double *f, const double *df, double *q, int precision);
 /* g = J(f)^T v: the vector-Jacobian product of Q at f; g_k = sum_i v_i dQ_i/df_k.
  * Adjoint of collision_mod.f90:213-216; equals 2*fmA*v at a Maxwellian
- * (collision_mod.f90:448-449, 357). */
+ * (collision_mod.f90:448-449, 357).  precision DGV_PREC_F64 or DGV_PREC_TC
+ * (as dgv_vjp_batched); DGV_PREC_F32C gives DGV_EUNSUP. */
 int dgv_vjp(dgv_ctx *ctx, const double *f, const double *v, double *g, int precision);
+/* The same for nb VDFs stored contiguously: g[b] = J(f[b])^T v[b].
+ * DGV_PREC_F64: the FP64 kernel per VDF.  DGV_PREC_TC: all VDFs in one pass
+ * of the block form on the tensor cores (8 or 27 nodes per cell): per
+ * cell-pair block the forward's product f(c2) W and the product f(c1) W'
+ * (the block's values with the two nodes' roles swapped), both contracted
+ * with c = 2v/w; split-fp16 operands, FP32 accumulation with compensated
+ * block sums, FP64 final sums.  The first call builds the adjoint's block
+ * records: twice the device memory of the forward's.  The reference has no
+ * adjoint: this is the transpose of the loop of collision_mod.f90:186-227,
+ * and 2*fmA*v of collision_mod.f90:448-449 at a Maxwellian. */
+int dgv_vjp_batched(dgv_ctx *ctx, int32_t nb, const double *f, const double *v, double *g, int precision);
 /* Stores the linearisation point fm (PrepareFMA_DGV, collision_mod.f90:377-464).
  * The dense N x N fmA is not materialised; dgv_apply_linear is matrix-free. */
 int dgv_prepare_linear(dgv_ctx *ctx, const double *fm);

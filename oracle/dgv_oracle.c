@@ -342,7 +342,7 @@ void dgvo_collide_aplus(const dgvo_ctx *c, const double *f, double *fc,
     if (!nodes) nnodes = c->N;
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
 #endif
     for (int64_t t = 0; t < nnodes; t++) {
         int64_t iphi = nodes ? nodes[t] : t;
@@ -1187,17 +1187,19 @@ int64_t dgvo_synth_A(const dgvo_ctx *c, uint64_t seed, double Trad, int support_
             pb[k] = (int32_t)i3; pd[k] = dsph; k++;
         }
     }
-    int32_t np_ = (p_only >= 0 && p_only < P) ? 1 : P;
+    /* one basis function (p_only) or all of them; with P = 1 both are p = 0 */
+    const int single = p_only >= 0 && p_only < P;
+    int32_t np_ = single ? 1 : P;
     int64_t nnz = npairs * np_;
     int32_t *capphi = calloc((size_t)N, sizeof(int32_t));
     double *A = malloc(sizeof(double) * (nnz ? nnz : 1));
     int32_t *X = malloc(sizeof(int32_t) * (nnz ? nnz : 1)), *X1 = malloc(sizeof(int32_t) * (nnz ? nnz : 1));
-    for (int32_t t = 0; t < np_; t++) capphi[(int64_t)cc * P + (np_ == 1 ? p_only : t)] = (int32_t)npairs;
+    for (int32_t t = 0; t < np_; t++) capphi[(int64_t)cc * P + (single ? p_only : t)] = (int32_t)npairs;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static)
 #endif
     for (int32_t t = 0; t < np_; t++) {
-        int32_t p = np_ == 1 ? p_only : t;
+        int32_t p = single ? p_only : t;
         int64_t base = (int64_t)t * npairs;
         for (int64_t i2 = 0; i2 < N; i2++)
             for (int64_t k = off[i2]; k < off[i2 + 1]; k++) {

@@ -100,3 +100,56 @@ def test_block_form_adjoint_equals_oracle_vjp(s, M, L, seed):
     g = g.ravel()
     ref = o.vjp(f, v)
     assert np.linalg.norm(g - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("s,M,L,seed", [(2, 3, 3.0, 5), (3, 3, 4.0, 9)])
+def test_adjoint_kernel_schedule_equals_oracle_vjp(s, M, L, seed):
+    """The schedule of the tensor-core adjoint kernel, restated: a CTA owns a
+    target cell T; each block (c1 <= c2) gives two items per valid output
+    cell D of its box (the per-axis bounds of the device layout):
+      pass 1: T = D + (c1 - cc) (linear indices), side = c(D), operand
+              f(D + c2 - cc), records W1[n = p*P + l1, k = l2];
+      pass 2: T = D + (c2 - cc), side = c(D), operand f(D + c1 - cc),
+              records W2[n = p*P + l2, k = l1];
+    and per row acc[n % P] += side[n / P] * (f W^T)[n], added to g(T).
+    Equals the oracle's VJP to 1e-13."""
+    from oracle.oracle import Oracle
+    o = Oracle(s, M, L)
+    cap, A, xi, xi1 = o.synth_A(seed=seed, support=1)
+    o.set_A(cap, A, xi, xi1)
+    P, Nc, cc = o.P, o.Nc, o.ccell
+    p = np.repeat(np.arange(o.N), cap) % P
+    assert np.all(xi < xi1)
+    blocks = {}
+    for k in range(len(A)):
+        W = blocks.setdefault((int(xi[k] // P), int(xi1[k] // P)), np.zeros((P, P, P)))
+        W[xi1[k] % P, xi[k] % P, p[k]] += A[k]
+    rng = np.random.default_rng(seed)
+    f = o.maxwellian(0.7, 0.4, 0.1, -0.2, 0.9) * (1.0 + 0.05 * rng.standard_normal(o.N))
+    v = rng.standard_normal(o.N)
+    fc = f.reshape(Nc, P)
+    cq = (2.0 * v / o.gwts).reshape(Nc, P)
+    c3 = _cell3(np.array(cc), M)
+    g = np.zeros((Nc, P))
+    for (a, b), W in blocks.items():
+        assert a <= b
+        e1, e2 = _cell3(np.array(a), M), _cell3(np.array(b), M)
+        lo = np.maximum(0, c3 - np.minimum(e1, e2))
+        hi = np.minimum(M - 1, c3 + M - 1 - np.maximum(e1, e2))
+        if np.any(hi < lo):
+            continue
+        W1 = W.transpose(2, 1, 0).reshape(P * P, P)   # [n = p*P + l1, k = l2]
+        W2 = W.transpose(2, 0, 1).reshape(P * P, P)   # [n = p*P + l2, k = l1]
+        o1, o2 = a - cc, b - cc
+        for u in range(lo[0], hi[0] + 1):
+            for vv in range(lo[1], hi[1] + 1):
+                for w in range(lo[2], hi[2] + 1):
+                    D = (u * M + vv) * M + w
+                    for T, opnd, Wr in ((D + o1, D + o2, W1), (D + o2, D + o1, W2)):
+                        G = Wr @ fc[opnd]                      # [n]
+                        acc = np.zeros(P)
+                        for n in range(P * P):
+                            acc[n % P] += cq[D, n // P] * G[n]
+                        g[T] += acc
+    ref = o.vjp(f, v)
+    assert np.linalg.norm(g.ravel() - ref) / np.linalg.norm(ref) < 1e-13
