@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libdgv_b200.so")
 DGV_OK, DGV_EINVAL, DGV_ERANGE, DGV_ECUDA, DGV_ETIMEOUT, DGV_ENOMEM, DGV_ESTATE, DGV_EUNSUP = range(8)
 DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC = 0, 1, 2
 DGV_OPT_PROJECT, DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM, DGV_OPT_TCTILES, DGV_OPT_TCSETMB = 1, 2, 3, 4, 5, 6
+DGV_OPT_WAIT_LIMIT_US, DGV_OPT_TEST_WITHHOLD = 7, 8
 
 STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4: "DGV_ETIMEOUT",
                 5: "DGV_ENOMEM", 6: "DGV_ESTATE", 7: "DGV_EUNSUP"}
@@ -24,7 +25,7 @@ EXPORTS = [
     "dgv_set_option", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper", "dgv_set_regime",
     "dgv_regime_info",
-    "dgv_step_rk", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
+    "dgv_step_rk", "dgv_step_rk_batched", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
     "dgv_jvp", "dgv_vjp", "dgv_vjp_batched", "dgv_prepare_linear", "dgv_apply_linear", "dgv_collide_f64_noalloc",
     "dgv_compute_A", "dgv_read_A_files", "dgv_write_A_file", "dgv_read_A_arrays", "dgv_write_A_arrays", "dgv_file_error",
     "dgv_write_solution", "dgv_read_solution", "dgv_write_solution_arrays", "dgv_read_solution_arrays",
@@ -87,6 +88,7 @@ def load() -> C.CDLL:
         "dgv_regime_info": [vp, C.POINTER(i32), C.POINTER(dbl)],
         "dgv_spatial_oper": [vp, vp, vp, dbl, C.c_int],
         "dgv_step_rk": [vp, vp, vp, dbl, C.c_int, C.c_int],
+        "dgv_step_rk_batched": [vp, i32, vp, vp, dbl, C.c_int, C.c_int],
         "dgv_prepare_ab": [vp, vp, dbl, C.c_int, C.c_int],
         "dgv_step_ab": [vp, vp, dbl, C.c_int],
         "dgv_write_solution": [vp, C.c_char_p, vp, dbl, dbl],

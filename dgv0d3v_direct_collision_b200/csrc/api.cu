@@ -346,6 +346,14 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
         ctx->c.tc_form = (int)value;
         release_graphs(&ctx->c);
         return DGV_OK;
+    case DGV_OPT_WAIT_LIMIT_US:
+        if (value < 0 || value > 60000000) return set_err(&ctx->c, DGV_EINVAL, "wait limit must be 0..60e6 us");
+        ctx->c.wait_limit_us = value;
+        release_graphs(&ctx->c);
+        return DGV_OK;
+    case DGV_OPT_TEST_WITHHOLD:
+        ctx->c.test_withhold = value != 0;
+        return DGV_OK;
     default: return set_err(&ctx->c, DGV_EINVAL, "unknown option");
     }
 }
@@ -542,6 +550,31 @@ int dgv_step_rk(dgv_ctx *ctx, double *f, double *frhs1, double dt, int order, in
     double *dr = rhost ? c->d_out + n : frhs1;
     if (!fdev) DGV_CUDA(c, cudaMemcpyAsync(df, f, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     TRY(rk_step_device(c, df, dr, dt, order, precision));
+    if (!fdev) DGV_CUDA(c, cudaMemcpyAsync(f, df, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (rhost) DGV_CUDA(c, cudaMemcpyAsync(frhs1, dr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (!fdev || rhost || !c->async) {
+        DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+        return check_errflag(c);
+    }
+    return DGV_OK;
+}
+
+// nb VDFs advanced in place; host arrays are staged in and copied back
+int dgv_step_rk_batched(dgv_ctx *ctx, int32_t nb, double *f, double *frhs1, double dt, int order, int precision)
+{
+    CTX_CHECK(ctx);
+    Ctx *c = &ctx->c;
+    if (!f || nb < 1) return set_err(c, DGV_EINVAL, "step_rk_batched: need nb >= 1 and a non-NULL f");
+    const size_t n = (size_t)nb * (size_t)c->grid.N;
+    bool fdev = false, rdev = false;
+    TRY(classify_ptr(c, f, &fdev));
+    if (frhs1) TRY(classify_ptr(c, frhs1, &rdev));
+    const bool rhost = frhs1 && !rdev;
+    if (!fdev || rhost) TRY(ensure_buffer(c, &c->d_out, &c->out_bytes, 2 * n * sizeof(double)));
+    double *df = fdev ? f : c->d_out;
+    double *dr = rhost ? c->d_out + n : frhs1;
+    if (!fdev) DGV_CUDA(c, cudaMemcpyAsync(df, f, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    TRY(rk_step_device(c, df, dr, dt, order, precision, nb));
     if (!fdev) DGV_CUDA(c, cudaMemcpyAsync(f, df, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (rhost) DGV_CUDA(c, cudaMemcpyAsync(frhs1, dr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (!fdev || rhost || !c->async) {

@@ -143,9 +143,10 @@ __device__ __forceinline__ float2 fmul2(float2 a, float2 b)
 
 // bounded wait whose outcome is the same for every lane of the warp (the
 // warp-collective tensor-memory instructions that follow need a converged warp)
-__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, int *err)
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, int *err,
+                                               unsigned long long limit_ns = WAIT_LIMIT_NS)
 {
-    const bool ok = mbar_wait(bar, parity, err);
+    const bool ok = mbar_wait(bar, parity, err, limit_ns);
     return __all_sync(0xffffffffu, ok);
 }
 
@@ -707,12 +708,15 @@ static int tc_work_lists(Ctx *c, int NDG, int key, const std::vector<int> &sets,
                 tc_items_for_block(g, bi, NDG, 0, (int)L.tc2_goff[b], msk, 27,
                                    t2_issued_cols(__builtin_popcount(msk) * g.P), bi.c1, bi.c2, per, work);
             } else {
-                const int o1 = bi.c1 - g.ccell, o2 = bi.c2 - g.ccell, full = (1 << g.P) - 1;
-                const long long wcol = t2_issued_cols(g.P * g.P);
-                // pass 1 (W1, to the c1 side): side cells T - o1, F16 cells T - o1 + o2
-                tc_items_for_block(g, bi, NDG, o1, b, full, 27, wcol, g.ccell - o1, g.ccell + o2 - o1, per, work);
+                const int o1 = bi.c1 - g.ccell, o2 = bi.c2 - g.ccell;
+                const int m1 = (int)L.tc2_mask[b], m2 = (int)L.tc2_mask[L.nblocks + b];
+                // pass 1 (W, to the c1 side): side cells T - o1, F16 cells T - o1 + o2
+                tc_items_for_block(g, bi, NDG, o1, (int)L.tc2_goff[b], m1, 27,
+                                   t2_issued_cols(__builtin_popcount(m1) * g.P), g.ccell - o1, g.ccell + o2 - o1,
+                                   per, work);
                 // pass 2 (W2, to the c2 side): side cells T - o2, F16 cells T - o2 + o1
-                tc_items_for_block(g, bi, NDG, o2, b | (1 << 30), full, 27, wcol, g.ccell - o2, g.ccell + o1 - o2,
+                tc_items_for_block(g, bi, NDG, o2, (int)L.tc2_goff2[b] | (1 << 30), m2, 27,
+                                   t2_issued_cols(__builtin_popcount(m2) * g.P), g.ccell - o2, g.ccell + o1 - o2,
                                    per, work);
             }
         }
@@ -789,6 +793,11 @@ constexpr int T2_GREC = 2 * T2_TILE;          // hi and lo tiles of one group
 constexpr int T2_NSTW = 3;                    // W ring stages
 constexpr int T2_ATILE = TC_ROWS * T2_K * 2;  // 128 rows x 32 fp16 (8 KiB)
 constexpr int T2_EPI_WARPS = 8;
+// slot header, after the side tile of the slot's first VDF tile: the item's
+// column count and, for each rank jj of its mask, the offset (floats) l*VB of
+// the node l in the side tile (-1 past the mask's nodes); written by the
+// producer before it arms the slot
+constexpr int T2_HDR = 128;
 constexpr int T2_THREADS = 32 * (2 + T2_EPI_WARPS);
 
 __host__ __device__ constexpr int t2_groups(int P) { return (P * P + T2_N - 1) / T2_N; }
@@ -809,43 +818,46 @@ __host__ __device__ __forceinline__ int t2_off(int row, int k)
     return ((row >> 3) * 4 + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-// per block the mask of the nodes l1 its pairs use (bit l1)
-__global__ void k_tc2_mask(const BlockInfo *blk, const double *rows64, int RD64, int Nc, int ccell, unsigned *mask)
+// per block the masks of the nodes l1 (mask[b]) and l2 (mask[nblocks + b])
+// its pairs use
+__global__ void k_tc2_mask(const BlockInfo *blk, const double *rows64, int RD64, int Nc, int ccell, unsigned *mask,
+                           long long nblocks)
 {
     const BlockInfo bi = blk[blockIdx.x];
-    unsigned m = 0u;
+    unsigned m1 = 0u, m2 = 0u;
     for (int k = threadIdx.x; k < bi.count; k += blockDim.x) {
         const long long o = __double_as_longlong(rows64[(size_t)(bi.start + k) * RD64]);
-        const int o1 = (int)(unsigned)(o & 0xffffffffLL);
-        m |= 1u << ((o1 - (bi.c1 - ccell)) / Nc);
+        const int o1 = (int)(unsigned)(o & 0xffffffffLL), o2 = (int)(o >> 32);
+        m1 |= 1u << ((o1 - (bi.c1 - ccell)) / Nc);
+        m2 |= 1u << ((o2 - (bi.c2 - ccell)) / Nc);
     }
-    m = __reduce_or_sync(0xffffffffu, m);
-    __shared__ unsigned sm[32];
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    m1 = __reduce_or_sync(0xffffffffu, m1);
+    m2 = __reduce_or_sync(0xffffffffu, m2);
+    __shared__ unsigned sm[2][32];
+    if ((threadIdx.x & 31) == 0) { sm[0][threadIdx.x >> 5] = m1; sm[1][threadIdx.x >> 5] = m2; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned r = 0u;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r |= sm[w];
-        mask[blockIdx.x] = r;
+        unsigned r1 = 0u, r2 = 0u;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) { r1 |= sm[0][w]; r2 |= sm[1][w]; }
+        mask[blockIdx.x] = r1;
+        mask[nblocks + blockIdx.x] = r2;
     }
 }
 
-// one record per block: t2_groups(P) groups of {W hi tile, W lo tile}, group
-// g holding columns n in [256 g, 256 g + 256) as tile rows.  Arrangement
-// 0 (collision operator): n = l1*P + p, K = l2.  The adjoint's: 1 (to the c1
-// side) n = p*P + l1, K = l2; 2 (to the c2 side) n = p*P + l2, K = l1.
-//
-// Arrangement 0 is compacted: only the nodes l1 of the block's mask get
-// columns, n = j*P + p with j = the rank of l1 in the mask, and the block's
-// record holds goff[b+1] - goff[b] = ceil(popc(mask) P / 256) groups from
-// group goff[b] on.  The adjoint's arrangements keep all P*P columns.
+// one record per block: groups of {W hi tile, W lo tile}, group g holding
+// columns n in [256 g, 256 g + 256) as tile rows, compacted to the nodes of
+// one of the block's masks: arrangement 0 (the collision operator and the
+// adjoint's pass to the c1 side) n = rank(l1)*P + p, K = l2, mask of the
+// nodes l1; arrangement 1 (the adjoint's pass to the c2 side) n = rank(l2)*P +
+// p, K = l1, mask of the nodes l2.  The block's record holds goff[b+1] -
+// goff[b] = ceil(popc(mask) P / 256) groups from group goff[b] on.
 __global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64, int P, int Nc, int ccell,
                             float vscale, unsigned char *W, int arr, const unsigned *mask, const long long *goff)
 {
     const BlockInfo bi = blk[blockIdx.x];
-    const int NG = arr == 0 ? (int)(goff[blockIdx.x + 1] - goff[blockIdx.x]) : t2_groups(P);
-    const unsigned msk = arr == 0 ? mask[blockIdx.x] : 0u;
-    unsigned char *rec = W + (arr == 0 ? (size_t)goff[blockIdx.x] : (size_t)blockIdx.x * NG) * T2_GREC;
+    const int NG = (int)(goff[blockIdx.x + 1] - goff[blockIdx.x]);
+    const unsigned msk = mask[blockIdx.x];
+    unsigned char *rec = W + (size_t)goff[blockIdx.x] * T2_GREC;
     uint4 *r4 = reinterpret_cast<uint4 *>(rec);
     for (int t = threadIdx.x; t < NG * T2_GREC / 16; t += blockDim.x) r4[t] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
@@ -855,9 +867,8 @@ __global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64
         const long long o = __double_as_longlong(row[0]);
         const int o1 = (int)(unsigned)(o & 0xffffffffLL), o2 = (int)(o >> 32);
         const int l1 = (o1 - (bi.c1 - ccell)) / Nc, l2 = (o2 - (bi.c2 - ccell)) / Nc;
-        const int lk = arr == 2 ? l1 : l2;
-        const int n = arr == 0 ? __popc(msk & ((1u << l1) - 1u)) * P + p : p * P + (arr == 2 ? l2 : l1);
-        const int g = n / T2_N;
+        const int lc = arr == 0 ? l1 : l2, lk = arr == 0 ? l2 : l1;
+        const int n = __popc(msk & ((1u << lc) - 1u)) * P + p, g = n / T2_N;
         const float x = (float)(row[1 + p] * (double)vscale);
         const __half h = __float2half_rn(x);
         const __half l = __float2half_rn(x - __half2float(h));
@@ -894,8 +905,8 @@ struct Tc2Args {
     const float *F;            // [nbt][Nc][P][VB] FP32 side factor: scaled f (forward) or c = 2v/w (adjoint)
     const unsigned char *F16;  // [nbt][hi, lo][Nc][VB x 32 tile]
     const unsigned char *W;    // block records
-    const unsigned char *W2;   // adjoint: records W2 (items with 1 << 30); W holds W1
-    const TcItem *items;       // work lists of this launch (chunk0 = block index, | 1 << 30 for W2)
+    const unsigned char *W2;   // adjoint: the records of its pass to the c2 side (items with 1 << 30)
+    const TcItem *items;       // work lists of this launch (chunk0 = first record group, | 1 << 30 for W2)
     const int *item_start;     // [ntiles + 1]
     const int *tile_of;        // row-tile index in launch order
     double *qacc;              // [(D*P+p)*NV + vdf]
@@ -903,7 +914,9 @@ struct Tc2Args {
     int *err;
     int Nc, ccell, NV, nvdf, nbt, nbp;
     int tpc;     // VDF tiles per CTA (1 or 2)
-    int region;  // bytes per VDF tile in an item slot: A hi, A lo, f(c1) (FP32)
+    int region;  // bytes per VDF tile in an item slot: A hi, A lo, side (FP32), slot header
+    unsigned long long wait_ns;  // limit of every bounded wait
+    int withhold;  // test of the bounded waits: CTA 0 withholds its first W copy
 };
 
 // MODE 0: Q(f,f), a CTA owns output cells D and an item (block c1, c2) reads
@@ -911,12 +924,15 @@ struct Tc2Args {
 //         per row acc[p] += f(c1+D, l1) G[(l1, p)].
 // MODE 1: the adjoint g = J(f)^T v (block form of the VJP), a CTA owns
 //         target cells T; an item is one of the two scatters of a block:
-//           W1 (pass 1, to the c1 side): G = f(c2+D) W1, D = T - c1,
+//           W  (pass 1, to the c1 side): G = f(c2+D) W,  D = T - c1,
 //           W2 (pass 2, to the c2 side): G = f(c1+D) W2, D = T - c2,
-//         its c1/c2 fields hold ccell + (side cell - T) and ccell + (F16
-//         cell - T); the side tile is c = 2v/w at cells D, the records'
-//         columns are p-major (n = p*P + l) and per row
-//         acc[l] += c(D, p) G[(p, l)], the forward's pattern.
+//         (W2: the block's values with the roles of its two nodes swapped,
+//         compacted to the nodes l2 of the block's second mask); the item's
+//         c1/c2 fields hold ccell + (side cell - T) and ccell + (F16 cell -
+//         T); the side tile is c = 2v/w at cells D, and per row each node l
+//         of the mask gets sum_p c(D, p) G[(rank(l), p)].
+// Both modes: an item's nch holds the block's node mask (low 27 bits) and the
+// owner cells it serves (bits 27..30), chunk0 its first record group.
 template <int VB, int P, int MODE>
 __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
 {
@@ -985,12 +1001,22 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             for (int it = i0; it < i1 && ok; it++) {
                 const TcItem e = a.items[it];
                 const int s = q & 1;
-                if (!mbar_wait(&s_empty[s], ((q >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
+                if (!mbar_wait(&s_empty[s], ((q >> 1) & 1) ^ 1, a.err, a.wait_ns)) { ok = false; break; }
                 // f of cells c1 + D - ccell (FP32) and c2 + D - ccell (fp16
                 // tiles), D in the row tile, clipped to the grid
                 const int cs1 = e.c1 + D0 - a.ccell, cs2 = e.c2 + D0 - a.ccell;
                 const int lo1 = max(cs1, 0), hi1 = min(cs1 + NDG, a.Nc);
                 const int lo2 = max(cs2, 0), hi2 = min(cs2 + NDG, a.Nc);
+                {
+                    int *hd = reinterpret_cast<int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE +
+                                                      NDG * P * VB * 4);
+                    const unsigned msk = (unsigned)e.nch & 0x7ffffffu;
+                    int k = 0;
+                    for (int l = 0; l < P; l++)
+                        if ((msk >> l) & 1u) hd[1 + k++] = l * VB;
+                    hd[0] = k * P;
+                    for (; k < P; k++) hd[1 + k] = -1;
+                }
                 uint32_t tx = 0;
                 if (hi1 > lo1) tx += (uint32_t)(nb2 * (hi1 - lo1) * P * VB * 4);
                 if (hi2 > lo2) tx += (uint32_t)(nb2 * 2 * (hi2 - lo2) * tile);
@@ -1014,23 +1040,23 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                     mbar_arrive(&s_full[s]);
                 }
                 q++;
-                // MODE 0: the block's compacted record (chunk0 = its first
-                // group); MODE 1: W1 or W2 of block chunk0 & 0x3fffffff
-                const int ngb = MODE == 0 ? t2_item_groups<P>(e.nch) : NG;
+                // the item's compacted record: groups from chunk0 & 0x3fffffff
+                // of W, or of W2 for the adjoint's pass to the c2 side
+                const int ngb = t2_item_groups<P>(e.nch);
                 const unsigned char *wrec =
-                    MODE == 0 ? a.W + (size_t)e.chunk0 * T2_GREC
-                              : ((e.chunk0 >> 30) ? a.W2 : a.W) + (size_t)(e.chunk0 & 0x3fffffff) * NG * T2_GREC;
+                    ((MODE == 1 && (e.chunk0 >> 30)) ? a.W2 : a.W) + (size_t)(e.chunk0 & 0x3fffffff) * T2_GREC;
                 for (int g = 0; g < ngb; g++, gw++) {
                     const int st = gw % T2_NSTW;
-                    if (!mbar_wait(&w_empty[st], ((gw / T2_NSTW) & 1) ^ 1, a.err)) { ok = false; break; }
+                    if (!mbar_wait(&w_empty[st], ((gw / T2_NSTW) & 1) ^ 1, a.err, a.wait_ns)) { ok = false; break; }
+                    if (a.withhold && blockIdx.x == 0 && gw == 0) continue;  // the stage nothing completes
                     mbar_arrive_expect_tx(&w_full[st], T2_GREC);
                     bulk_g2s(wring + st * T2_GREC, wrec + (size_t)g * T2_GREC, T2_GREC, &w_full[st]);
                 }
             }
             if (!ok) {  // let the copies already issued land
                 for (int j = gw > T2_NSTW ? gw - T2_NSTW : 0; j < gw; j++)
-                    mbar_wait(&w_full[j % T2_NSTW], (j / T2_NSTW) & 1, a.err);
-                for (int j = q > 2 ? q - 2 : 0; j < q; j++) mbar_wait(&s_full[j & 1], (j >> 1) & 1, a.err);
+                    mbar_wait(&w_full[j % T2_NSTW], (j / T2_NSTW) & 1, a.err, a.wait_ns);
+                for (int j = q > 2 ? q - 2 : 0; j < q; j++) mbar_wait(&s_full[j & 1], (j >> 1) & 1, a.err, a.wait_ns);
             }
         }
         __syncwarp();
@@ -1045,20 +1071,21 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             bool ok = true;
             for (int it = i0; it < i1 && ok; it++) {
                 const int s = q & 1;
-                const int ncol = MODE == 0 ? __popc((unsigned)a.items[it].nch & 0x7ffffffu) * P : P * P;
+                if (!mbar_wait(&s_full[s], (q >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
+                const int ncol = *reinterpret_cast<const int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE +
+                                                                 NDG * P * VB * 4);
                 const int ngb = (ncol + T2_N - 1) / T2_N;
                 const int nlast = ((ncol - (ngb - 1) * T2_N) + 15) / 16 * 16;
                 const uint32_t idesc_last = (1u << 4) | ((uint32_t)(nlast >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
-                if (!mbar_wait(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
                 for (int g = 0; g < ngb && ok; g++, gw++) {
                     const int st = gw % T2_NSTW;
-                    if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err)) { ok = false; break; }
+                    if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err, a.wait_ns)) { ok = false; break; }
                     const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
                     const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
                     const uint32_t id = g == ngb - 1 ? idesc_last : idesc;
                     for (int j = 0; j < nb2; j++, J++) {
                         const int cs = J & 1;
-                        if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, a.err)) { ok = false; break; }
+                        if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, a.err, a.wait_ns)) { ok = false; break; }
                         tc_fence_after();
                         unsigned char *reg = slots + (size_t)(2 * s + j) * a.region;
                         const uint64_t dAh = umma_desc(smem_u32(reg), 128, 512);
@@ -1081,7 +1108,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             }
             // every MMA issued so far completes before tensor memory is freed
             umma_commit(drain);
-            mbar_wait(drain, 0, a.err);
+            mbar_wait(drain, 0, a.err, a.wait_ns);
         }
         __syncwarp();
     } else if ((warp - 2) / 4 < nb2) {
@@ -1098,57 +1125,65 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             const int nch = a.items[it].nch;
             const bool valid = (nch >> (27 + d)) & 1;
             const unsigned msk = (unsigned)nch & 0x7ffffffu;
-            const int nl = MODE == 0 ? __popc(msk) : P, ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
+            const int nl = __popc(msk), ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
             const int s = q & 1;
-            if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err)) { ok = false; break; }
+            if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
             const float *f1s =
                 reinterpret_cast<const float *>(slots + (size_t)(2 * s + j) * a.region + 2 * T2_ATILE) + d * P * VB + v;
-            // side factor of the item's rows: f(c1 + D, l1) for the j-th node
-            // l1 of the mask (MODE 0, columns n = j*P + p; 0 for j past the
-            // mask's nodes) or c(D, p) (MODE 1, columns n = p*P + l); either
-            // way acc[n % P] += side[n / P] * G[n]
-            // (MODE 0 loads each factor at its first column: all 27 live at
-            // once, with the mask lookups, would spill)
-            float f1[P], acc[P], fcur = 0.f;
+            const int *hoff =
+                reinterpret_cast<const int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE + NDG * P * VB * 4) + 1;
+            // Columns n = jj*P + p, jj = the rank of a node of the item's mask.
+            // MODE 0: side = f(c1 + D, l1) of the jj-th node l1 (its offset from
+            //         the slot header), loaded at its first column (all 27 live
+            //         at once would spill), acc[p] += side * G[n].
+            // MODE 1: side = c(D, p) (all P live), the sum over p of each jj is
+            //         complete after its P consecutive columns and is kept in
+            //         stg[jj] (local memory: its read index is the rank of a
+            //         node); after the item each node l of the mask adds
+            //         stg[rank(l)] into its (sum, correction).
+            float f1[MODE == 1 ? P : 1], acc[MODE == 0 ? P : 1], stg[MODE == 1 ? P : 1], fcur = 0.f, run = 0.f;
 #pragma unroll
             for (int l = 0; l < P; l++) {
-                if (MODE == 1) f1[l] = f1s[l * VB];
-                acc[l] = 0.f;
+                if constexpr (MODE == 1) f1[l] = f1s[l * VB];
+                else acc[l] = 0.f;
             }
+            // MODE 0: two 32-column loads per wait (the load latency is paid four
+            // times per 256-column group); MODE 1 keeps more values live: one
+            constexpr int LW = MODE == 0 ? 64 : 32;
 #pragma unroll
             for (int g = 0; g < NG; g++) {
                 if (g >= ngb) break;
                 const int J = (gq + g) * nb2 + j, cs = J & 1;
-                if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, a.err)) { ok = false; break; }
+                if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
                 tc_fence_after();
-                // two 32-column loads per wait: the load latency is paid
-                // four times per 256-column group
 #pragma unroll
-                for (int hh = 0; hh < T2_N / 64; hh++) {
-                    if (g * T2_N + 64 * hh >= P * P || g * T2_N + 64 * hh >= ncol) break;
-                    uint32_t G[64];
-                    tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh), G);
-                    if (g * T2_N + 64 * hh + 32 < P * P) {
-                        if (g * T2_N + 64 * hh + 32 < ncol) {
-                            tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + 64 * hh + 32), G + 32);
+                for (int hh = 0; hh < T2_N / LW; hh++) {
+                    if (g * T2_N + LW * hh >= P * P || g * T2_N + LW * hh >= ncol) break;
+                    uint32_t G[LW];
+                    tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + LW * hh), G);
+                    if (LW == 64 && g * T2_N + LW * hh + 32 < P * P) {
+                        if (g * T2_N + LW * hh + 32 < ncol) {
+                            tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + LW * hh + 32), G + 32);
                         } else {
 #pragma unroll
-                            for (int i = 32; i < 64; i++) G[i] = 0u;
+                            for (int i = 32; i < LW; i++) G[i] = 0u;
                         }
                     }
                     tmem_wait_ld();
 #pragma unroll
-                    for (int i = 0; i < 64; i++) {
-                        const int n = g * T2_N + 64 * hh + i;
+                    for (int i = 0; i < LW; i++) {
+                        const int n = g * T2_N + LW * hh + i;
                         if (n < P * P) {
                             if constexpr (MODE == 0) {
                                 if (n % P == 0 || i == 0) {
-                                    const int jj = n / P;
-                                    fcur = jj < nl ? f1s[__fns(msk, 0u, jj + 1) * VB] : 0.f;
+                                    const int o = hoff[n / P];
+                                    fcur = o >= 0 ? f1s[o] : 0.f;
                                 }
                                 acc[n % P] = fmaf(fcur, __uint_as_float(G[i]), acc[n % P]);
                             } else {
-                                acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
+                                run = n % P == 0 ? f1[0] * __uint_as_float(G[i])
+                                                 : fmaf(f1[n % P], __uint_as_float(G[i]), run);
+                                if (n % P == P - 1) stg[n / P] = run;
                             }
                         }
                     }
@@ -1164,8 +1199,15 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             if (valid) {
 #pragma unroll
                 for (int p = 0; p < P; p++) {  // two-sum of the block total into (sum, correction)
-                    const float t = S[p] + acc[p], bpv = t - S[p];
-                    Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
+                    float x;
+                    if constexpr (MODE == 0) {
+                        x = acc[p];
+                    } else {
+                        if (!((msk >> p) & 1u)) continue;
+                        x = stg[__popc(msk & ((1u << p) - 1u))];
+                    }
+                    const float t = S[p] + x, bpv = t - S[p];
+                    Cc[p] += (S[p] - (t - bpv)) + (x - bpv);
                     S[p] = t;
                 }
             }
@@ -1201,15 +1243,17 @@ static int tc2_prepare(Ctx *c)
     int rc = tc_value_scale(c, &L.tc2_vscale);
     if (rc) return rc;
     const long long nb = L.nblocks;
-    L.tc2_mask.assign((size_t)nb, 0u);
+    L.tc2_mask.assign(2 * (size_t)nb, 0u);
     L.tc2_goff.assign((size_t)nb + 1, 0);
     unsigned *d_mask = nullptr;
     long long *d_goff = nullptr;
-    DGV_CUDA(c, cudaMalloc(&d_mask, sizeof(unsigned) * std::max<long long>(1, nb)));
+    DGV_CUDA(c, cudaMalloc(&d_mask, sizeof(unsigned) * std::max<long long>(1, 2 * nb)));
     if (nb) {
-        k_tc2_mask<<<(unsigned)nb, 128, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.Nc, g.ccell, d_mask);
+        k_tc2_mask<<<(unsigned)nb, 128, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.Nc, g.ccell, d_mask,
+                                                         nb);
         DGV_CUDA(c, cudaGetLastError());
-        DGV_CUDA(c, cudaMemcpyAsync(L.tc2_mask.data(), d_mask, sizeof(unsigned) * nb, cudaMemcpyDeviceToHost, c->stream));
+        DGV_CUDA(c, cudaMemcpyAsync(L.tc2_mask.data(), d_mask, sizeof(unsigned) * 2 * nb, cudaMemcpyDeviceToHost,
+                                    c->stream));
         DGV_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     for (long long b = 0; b < nb; b++)
@@ -1268,6 +1312,16 @@ static void tc2_sets(Ctx *c)
     L.tc2_set_mb = c->tc_set_mb;
 }
 
+// the wait limit of the launches, and the one-shot test switch (DGV_OPT_TEST_WITHHOLD:
+// CTA 0 of the first launch arms no copy for its first W stage, so the waits on
+// that stage run out and the call reports DGV_ETIMEOUT)
+static void tc2_wait_args(Ctx *c, Tc2Args &a)
+{
+    a.wait_ns = c->wait_limit_us > 0 ? (unsigned long long)c->wait_limit_us * 1000ULL : WAIT_LIMIT_NS;
+    a.withhold = c->test_withhold ? 1 : 0;
+    c->test_withhold = false;
+}
+
 template <int VB, int P, int MODE = 0>
 static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng)
 {
@@ -1281,6 +1335,7 @@ static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng)
         a.tile_of = tl.tile_of + s * ng;
         k_collide_tc2<VB, P, MODE><<<(unsigned)(a.nbp * ng), T2_THREADS, smem, c->stream>>>(a);
         DGV_CUDA(c, cudaGetLastError());
+        a.withhold = 0;  // the test withholds in the first launch only
     }
     kt.stop((long long)L.tc2_sets.size() - 1);
     count_launches(c, (long long)L.tc2_sets.size() - 1);
@@ -1335,7 +1390,8 @@ static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, 
     a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
     a.tpc = c->tc_tiles_per_cta;
     a.nbp = (nbt + a.tpc - 1) / a.tpc;
-    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + 1023) / 1024 * 1024;
+    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
+    tc2_wait_args(c, a);
     rc = g.P == 27 ? launch_tc2_vb<27>(c, a, tl, ng, VB) : launch_tc2_vb<8>(c, a, tl, ng, VB);
     if (rc) return rc;
     long long tot = (long long)nvdf * g.N;
@@ -1403,29 +1459,41 @@ __global__ void k_tc_vjp_final(const double *gacc, const double *inv_f, const do
     g[(size_t)v * N + i] = gacc[i * NV + v] * inv_f[v] * inv_c[v];
 }
 
-// the adjoint's block records W1 and W2 (arrangements 1 and 2 of
-// k_tc2_build), built on the first adjoint call with the value scale of W
+// the adjoint's second record set W2 (arrangement 1 of k_tc2_build, compacted
+// to the blocks' masks of nodes l2), built on the first adjoint call with the
+// value scale of W; the pass to the c1 side reads W itself
 static int tc2_prepare_adjoint(Ctx *c)
 {
     Layout &L = c->lay;
-    if (L.tc2_Wv[0] && L.tc2_Wv[1]) return DGV_OK;
+    if (L.tc2_Wv) return DGV_OK;
     const Grid &g = c->grid;
-    const size_t rec = (size_t)t2_groups(g.P) * T2_GREC;
-    for (int k = 0; k < 2; k++) {
-        if (L.tc2_Wv[k]) continue;
-        cudaError_t e = cudaMalloc(&L.tc2_Wv[k], (size_t)std::max<long long>(1, L.nblocks) * rec);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            L.tc2_Wv[k] = nullptr;
-            return set_err(c, DGV_ENOMEM, "tensor-core adjoint: no room for its block records");
-        }
-        if (L.nblocks)
-            k_tc2_build<<<(unsigned)L.nblocks, 256, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.P,
-                                                                     g.Nc, g.ccell, (float)L.tc2_vscale,
-                                                                     (unsigned char *)L.tc2_Wv[k], k + 1, nullptr,
-                                                                     nullptr);
-        DGV_CUDA(c, cudaGetLastError());
+    const long long nb = L.nblocks;
+    L.tc2_goff2.assign((size_t)nb + 1, 0);
+    for (long long b = 0; b < nb; b++)
+        L.tc2_goff2[b + 1] = L.tc2_goff2[b] + (__builtin_popcount(L.tc2_mask[nb + b]) * g.P + T2_N - 1) / T2_N;
+    unsigned *d_mask = nullptr;
+    long long *d_goff = nullptr;
+    cudaError_t e = cudaMalloc(&L.tc2_Wv, (size_t)std::max<long long>(1, L.tc2_goff2[nb]) * T2_GREC);
+    if (e != cudaSuccess || cudaMalloc(&d_mask, sizeof(unsigned) * std::max<long long>(1, nb)) != cudaSuccess ||
+        cudaMalloc(&d_goff, sizeof(long long) * (nb + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        if (L.tc2_Wv) cudaFree(L.tc2_Wv);
+        if (d_mask) cudaFree(d_mask);
+        L.tc2_Wv = nullptr;
+        return set_err(c, DGV_ENOMEM, "tensor-core adjoint: no room for its block records");
     }
+    DGV_CUDA(c, cudaMemcpyAsync(d_mask, L.tc2_mask.data() + nb, sizeof(unsigned) * nb, cudaMemcpyHostToDevice,
+                                c->stream));
+    DGV_CUDA(c, cudaMemcpyAsync(d_goff, L.tc2_goff2.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice,
+                                c->stream));
+    if (nb)
+        k_tc2_build<<<(unsigned)nb, 256, 0, c->stream>>>(L.blk, (const double *)L.rows64, L.RD64, g.P, g.Nc, g.ccell,
+                                                          (float)L.tc2_vscale, (unsigned char *)L.tc2_Wv, 1, d_mask,
+                                                          d_goff);
+    DGV_CUDA(c, cudaGetLastError());
+    DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(d_mask);
+    cudaFree(d_goff);
     return DGV_OK;
 }
 
@@ -1470,12 +1538,13 @@ int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, gbytes, c->stream));
     Tc2Args a;
-    a.F = Cf; a.F16 = F16; a.W = (const unsigned char *)L.tc2_Wv[0]; a.W2 = (const unsigned char *)L.tc2_Wv[1];
+    a.F = Cf; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.W2 = (const unsigned char *)L.tc2_Wv;
     a.items = tl.items; a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = nullptr;
     a.err = c->d_err; a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
     a.tpc = c->tc_tiles_per_cta;
     a.nbp = (nbt + a.tpc - 1) / a.tpc;
-    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + 1023) / 1024 * 1024;
+    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
+    tc2_wait_args(c, a);
     rc = g.P == 27 ? launch_tc2_vb<27, 1>(c, a, tl, ng, VB) : launch_tc2_vb<8, 1>(c, a, tl, ng, VB);
     if (rc) return rc;
     const long long tot = (long long)nvdf * g.N;

@@ -74,7 +74,7 @@ struct Layout {
     // block form (built on first use): per block the dense split-fp16 tiles
     // W[l2][(l1, p)] of its values, the value scale, and the block sets
     void *tc2_W = nullptr;  // device
-    void *tc2_Wv[2] = {nullptr, nullptr};  // device: the adjoint's records (built on first use)
+    void *tc2_Wv = nullptr;  // device: the adjoint's second record set (built on first use)
     double tc2_vscale = 1.0;
     std::vector<int> tc2_sets;
     int tc2_set_mb = 0;  // record megabytes per set the sets were built for
@@ -83,11 +83,13 @@ struct Layout {
     std::map<int, std::vector<void *>> tc_lists;
     std::map<int, long long> tc_list_work;   // per key: sum of the items' work (chunk records / issued columns)
     std::map<int, long long> tc_list_items;  // per key: number of items
-    // block form: per block the mask of its nodes l1 (bit l1 set if the
-    // block has a pair with it) and the first record group of the block's
-    // compacted records (nblocks + 1 entries, host)
+    // block form: per block the masks of its nodes l1 (entries 0..nblocks-1)
+    // and l2 (nblocks..2 nblocks-1; bit l set if the block has a pair with
+    // node l) and the first record group of the block's compacted records in
+    // W (tc2_goff) and in the adjoint's W2 (tc2_goff2); nblocks + 1 entries,
+    // host
     std::vector<uint32_t> tc2_mask;
-    std::vector<long long> tc2_goff;
+    std::vector<long long> tc2_goff, tc2_goff2;
 };
 void free_layout(Layout &L);
 
@@ -140,6 +142,8 @@ struct Ctx {
     int tc_form = 2;  // DGV_OPT_TCFORM: 1 chunk form, 2 block form (8 or 27 nodes per cell)
     int tc_tiles_per_cta = 2;  // DGV_OPT_TCTILES: VDF tiles per CTA in the block form
     int tc_set_mb = 48;        // DGV_OPT_TCSETMB: block form, MB of records per launch
+    long long wait_limit_us = 0;  // DGV_OPT_WAIT_LIMIT_US: bounded waits of the block form (0 = 4 s)
+    bool test_withhold = false;   // DGV_OPT_TEST_WITHHOLD: the next block-form launch withholds one copy
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
     long long kt_launches = 0, kt_all = 0;
     double kt_ms = 0.0;
@@ -198,7 +202,7 @@ int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int
 int moments_device(Ctx *c, const double *d_f, int nvdf, double *h_out);
 int project_device(Ctx *c, double *d_q, int nvdf);
 int maxwellian_device(Ctx *c, double T, double u0, double v0, double w0, double n, double *d_f);
-int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, int precision);
+int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, int precision, int nb = 1);
 int spatial_device(Ctx *c, const double *d_f, double *d_out, double dt, int precision);
 int ab_prepare_device(Ctx *c, double *d_f, double dt, int order, int precision);
 int ab_step_device(Ctx *c, double *d_f, double dt, int precision);

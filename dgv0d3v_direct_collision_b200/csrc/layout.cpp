@@ -29,8 +29,7 @@ void free_layout(Layout &L)
     if (L.tc_V) cudaFree(L.tc_V);
     if (L.tc_chunk_start) cudaFree(L.tc_chunk_start);
     if (L.tc2_W) cudaFree(L.tc2_W);
-    for (void *w : L.tc2_Wv)
-        if (w) cudaFree(w);
+    if (L.tc2_Wv) cudaFree(L.tc2_Wv);
     for (auto &kv : L.tc_lists)
         for (void *p : kv.second) cudaFree(p);
     L = Layout();

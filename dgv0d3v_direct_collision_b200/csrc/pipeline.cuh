@@ -56,14 +56,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 // waiting it also looks at the error flag about once a millisecond, so once
 // one wait has given up the other waits of the launch (and of launches queued
 // behind it) give up within a millisecond instead of each running its limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err,
+                                          unsigned long long limit_ns = WAIT_LIMIT_NS)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     unsigned long long tcheck = t0;
     while (!mbar_try_wait(bar, parity)) {
         const unsigned long long t = globaltimer_ns();
-        if (t - t0 > WAIT_LIMIT_NS) {
+        if (t - t0 > limit_ns) {
             *(volatile int *)err = 1;  // host-mapped flag, read after the stream synchronises
             return false;
         }

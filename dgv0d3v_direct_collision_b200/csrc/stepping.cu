@@ -219,25 +219,41 @@ __global__ void k_stage(StageArgs a)
     a.out[i] = y;
 }
 
+// the stage combination over the nb VDFs of a batch (nb * N entries; the
+// coefficients do not depend on the VDF)
+static int stage_nb(Ctx *c, int nb, int op, double *out, const double *f, const double *r1,
+                    const double *t2 = nullptr, const double *t3 = nullptr, const double *t4 = nullptr,
+                    double dt = 1.0, const double *h2 = nullptr, const double *h3 = nullptr,
+                    const double *h4 = nullptr, const double *h5 = nullptr)
+{
+    StageArgs a;
+    a.f = f; a.r1 = r1; a.t2 = t2; a.t3 = t3; a.t4 = t4; a.h2 = h2; a.h3 = h3; a.h4 = h4; a.h5 = h5;
+    a.out = out; a.n = (long long)nb * c->grid.N; a.dt = dt; a.op = op;
+    k_stage<<<(unsigned)((a.n + 255) / 256), 256, 0, c->stream>>>(a);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 1);
+    return DGV_OK;
+}
+
 static int stage(Ctx *c, int op, double *out, const double *f, const double *r1, const double *t2 = nullptr,
                  const double *t3 = nullptr, const double *t4 = nullptr, double dt = 1.0,
                  const double *h2 = nullptr, const double *h3 = nullptr, const double *h4 = nullptr,
                  const double *h5 = nullptr)
 {
-    StageArgs a;
-    a.f = f; a.r1 = r1; a.t2 = t2; a.t3 = t3; a.t4 = t4; a.h2 = h2; a.h3 = h3; a.h4 = h4; a.h5 = h5;
-    a.out = out; a.n = c->grid.N; a.dt = dt; a.op = op;
-    k_stage<<<(unsigned)((a.n + 255) / 256), 256, 0, c->stream>>>(a);
-    DGV_CUDA(c, cudaGetLastError());
-    return DGV_OK;
+    return stage_nb(c, 1, op, out, f, r1, t2, t3, t4, dt, h2, h3, h4, h5);
 }
 
-static int ensure_tmp(Ctx *c)
+// the RK temporaries, for batches of up to nb VDFs; growing them releases
+// the graphs that captured the old ones
+static int ensure_tmp(Ctx *c, int nb = 1)
 {
-    if (c->tmp_n == (size_t)c->grid.N && c->d_tmp[0]) return DGV_OK;
+    const size_t need = (size_t)nb * (size_t)c->grid.N;
+    if (c->tmp_n >= need && c->d_tmp[0]) return DGV_OK;
+    release_graphs(c);
     for (auto &p : c->d_tmp) { if (p) cudaFree(p); p = nullptr; }
-    for (auto &p : c->d_tmp) DGV_CUDA(c, cudaMalloc(&p, sizeof(double) * (size_t)c->grid.N));
-    c->tmp_n = (size_t)c->grid.N;
+    c->tmp_n = 0;
+    for (auto &p : c->d_tmp) DGV_CUDA(c, cudaMalloc(&p, sizeof(double) * need));
+    c->tmp_n = need;
     return DGV_OK;
 }
 
@@ -360,58 +376,68 @@ static int spatial(Ctx *c, const double *x, double *out, double dt, int precisio
     return spatial_device(c, x, out, dt, precision);
 }
 
-// one RK step of the given order; d_r1 receives frhs1 (already divided by dt)
-static int rk_body(Ctx *c, double *f, double *r1, double dt, int order, int precision)
+// one RK step of the given order for nb VDFs; d_r1 receives frhs1 (already
+// divided by dt).  A batch evaluates Q of all its VDFs in one call per stage
+// (run modes are per VDF and need nb = 1).
+static int rk_body(Ctx *c, double *f, double *r1, double dt, int order, int precision, int nb = 1)
 {
     double *t0 = c->d_tmp[0], *t2 = c->d_tmp[1], *t3 = c->d_tmp[2], *t4 = c->d_tmp[3];
+    auto spatial = [c, nb](const double *x, double *out, double dt_, int prec) {
+        return nb == 1 ? spatial_device(c, x, out, dt_, prec)
+                       : collide_device(c, x, out, nb, prec, c->grid.d.kappa * dt_);
+    };
+    auto stage = [c, nb](int op, double *out, const double *f_, const double *r1_, const double *t2_ = nullptr,
+                         const double *t3_ = nullptr, const double *t4_ = nullptr, double dt_ = 1.0) {
+        return stage_nb(c, nb, op, out, f_, r1_, t2_, t3_, t4_, dt_);
+    };
     switch (order) {
     case 1:
-        TRY(spatial(c, f, r1, dt, precision));
-        TRY(stage(c, RK1_F, f, f, r1));
+        TRY(spatial(f, r1, dt, precision));
+        TRY(stage(RK1_F, f, f, r1));
         break;
     case 2:
-        TRY(spatial(c, f, r1, dt, precision));
-        TRY(stage(c, RK2_T2, t0, f, r1));
-        TRY(spatial(c, t0, t2, dt, precision));
-        TRY(stage(c, RK2_F, f, f, r1, t2));
+        TRY(spatial(f, r1, dt, precision));
+        TRY(stage(RK2_T2, t0, f, r1));
+        TRY(spatial(t0, t2, dt, precision));
+        TRY(stage(RK2_F, f, f, r1, t2));
         break;
     case 3:
-        TRY(spatial(c, f, r1, dt, precision));
-        TRY(stage(c, RK3_T2, t0, f, r1));
-        TRY(spatial(c, t0, t2, dt, precision));
-        TRY(stage(c, RK3_T3, t0, f, r1, t2));
-        TRY(spatial(c, t0, t3, dt, precision));
-        TRY(stage(c, RK3_F, f, f, r1, t2, t3));
+        TRY(spatial(f, r1, dt, precision));
+        TRY(stage(RK3_T2, t0, f, r1));
+        TRY(spatial(t0, t2, dt, precision));
+        TRY(stage(RK3_T3, t0, f, r1, t2));
+        TRY(spatial(t0, t3, dt, precision));
+        TRY(stage(RK3_F, f, f, r1, t2, t3));
         break;
     case 4:
-        TRY(spatial(c, f, r1, dt, precision));
-        TRY(stage(c, RK4_T2, t0, f, r1));
-        TRY(spatial(c, t0, t2, dt, precision));
-        TRY(stage(c, RK4_T3, t0, f, r1, t2));
-        TRY(spatial(c, t0, t3, dt, precision));
-        TRY(stage(c, RK4_T4, t0, f, r1, t2, t3));
-        TRY(spatial(c, t0, t2, dt, precision));  // the 4th stage reuses ft2 (:102)
-        TRY(stage(c, RK4_F, f, f, r1, t2, t3));
+        TRY(spatial(f, r1, dt, precision));
+        TRY(stage(RK4_T2, t0, f, r1));
+        TRY(spatial(t0, t2, dt, precision));
+        TRY(stage(RK4_T3, t0, f, r1, t2));
+        TRY(spatial(t0, t3, dt, precision));
+        TRY(stage(RK4_T4, t0, f, r1, t2, t3));
+        TRY(spatial(t0, t2, dt, precision));  // the 4th stage reuses ft2 (:102)
+        TRY(stage(RK4_F, f, f, r1, t2, t3));
         break;
     case 5:
-        TRY(spatial(c, f, r1, dt, precision));
-        TRY(stage(c, RK5_T2, t0, f, r1));
-        TRY(spatial(c, t0, t2, dt, precision));
-        TRY(stage(c, RK5_T3, t0, f, r1, t2));
-        TRY(spatial(c, t0, t3, dt, precision));
-        TRY(stage(c, RK5_T4, t0, f, r1, t2, t3));
-        TRY(spatial(c, t0, t4, dt, precision));
-        TRY(stage(c, RK5_FT3, t3, nullptr, nullptr, t2, t3));
-        TRY(stage(c, RK5_T5, t0, f, r1, t2, t3, t4));
-        TRY(spatial(c, t0, t2, dt, precision));  // ft5 kept in ft2 (:136)
-        TRY(stage(c, RK5_T6, t0, f, r1, t2, t3, t4));
-        TRY(spatial(c, t0, t3, dt, precision));  // ft6 kept in ft3 (:140)
-        TRY(stage(c, RK5_F, f, f, r1, t2, t3, t4));
+        TRY(spatial(f, r1, dt, precision));
+        TRY(stage(RK5_T2, t0, f, r1));
+        TRY(spatial(t0, t2, dt, precision));
+        TRY(stage(RK5_T3, t0, f, r1, t2));
+        TRY(spatial(t0, t3, dt, precision));
+        TRY(stage(RK5_T4, t0, f, r1, t2, t3));
+        TRY(spatial(t0, t4, dt, precision));
+        TRY(stage(RK5_FT3, t3, nullptr, nullptr, t2, t3));
+        TRY(stage(RK5_T5, t0, f, r1, t2, t3, t4));
+        TRY(spatial(t0, t2, dt, precision));  // ft5 kept in ft2 (:136)
+        TRY(stage(RK5_T6, t0, f, r1, t2, t3, t4));
+        TRY(spatial(t0, t3, dt, precision));  // ft6 kept in ft3 (:140)
+        TRY(stage(RK5_F, f, f, r1, t2, t3, t4));
         break;
     default:
         return set_err(c, DGV_EINVAL, "step_rk: order must be 1..5");
     }
-    TRY(stage(c, DIV_DT, r1, nullptr, r1, nullptr, nullptr, nullptr, dt));
+    TRY(stage(DIV_DT, r1, nullptr, r1, nullptr, nullptr, nullptr, dt));
     return DGV_OK;
 }
 
@@ -421,7 +447,7 @@ static int rk_body(Ctx *c, double *f, double *r1, double dt, int order, int prec
 struct RkGraphKey {
     double *f, *r1;
     double dt;
-    int order, precision, project;
+    int order, precision, project, nb;
     bool operator<(const RkGraphKey &o) const
     {
         return std::memcmp(this, &o, sizeof(*this)) < 0;
@@ -448,10 +474,13 @@ void release_graphs(const Ctx *c)
     g_graphs.erase(it);
 }
 
-int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, int precision)
+int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, int precision, int nb)
 {
     if (order < 1 || order > 5) return set_err(c, DGV_EINVAL, "step_rk: order must be 1..5");
-    TRY(ensure_tmp(c));
+    if (nb < 1) return set_err(c, DGV_EINVAL, "step_rk: batch must hold at least one VDF");
+    if (nb > 1 && c->decomp_lev > 0.0)
+        return set_err(c, DGV_EUNSUP, "step_rk: run modes (dgv_set_regime) are per VDF; batches need them off");
+    TRY(ensure_tmp(c, nb));
     double *r1 = d_frhs1 ? d_frhs1 : c->d_tmp[4];
     // with run modes the mode check synchronises on the host at every stage:
     // no graph capture
@@ -459,6 +488,7 @@ int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, i
     RkGraphKey key;
     std::memset(&key, 0, sizeof(key));
     key.f = d_f; key.r1 = r1; key.dt = dt; key.order = order; key.precision = precision; key.project = c->project;
+    key.nb = nb;
     std::unique_lock<std::recursive_mutex> lk(g_graphs_mu);
     RkGraph &gr = g_graphs[c][key];
     if (gr.exec) {
@@ -466,11 +496,11 @@ int rk_step_device(Ctx *c, double *d_f, double *d_frhs1, double dt, int order, i
         count_launches(c, gr.launches);
         return DGV_OK;
     }
-    if (gr.calls++ == 0) return rk_body(c, d_f, r1, dt, order, precision);
+    if (gr.calls++ == 0) return rk_body(c, d_f, r1, dt, order, precision, nb);
     const long long before = c->kt_all;
     cudaGraph_t graph = nullptr;
     DGV_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = rk_body(c, d_f, r1, dt, order, precision);
+    int rc = rk_body(c, d_f, r1, dt, order, precision, nb);
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
     if (e != cudaSuccess) return set_err(c, DGV_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));

@@ -302,11 +302,20 @@ class DGVSolver:
 
     # -- time integration ----------------------------------------------------
     def TimeIntegratorORK_SH_DGV(self, f, dt, frhs1=None, order=None, precision=None):
-        """One RK step in place on f; returns frhs1 (first-stage right side / dt)."""
+        """One RK step in place on f, one VDF [N] or a batch [nb, N]
+        (dgv_step_rk_batched: each stage's Q of the batch in one call);
+        returns frhs1 (first-stage right side / dt)."""
         _check_f64(f)
+        if f.shape[-1] != self.N:
+            raise ValueError("TimeIntegratorORK_SH_DGV: last axis must have N entries")
         frhs1 = self._like(f) if frhs1 is None else frhs1
-        self._check(self._lib.dgv_step_rk(self._h, _ptr(f), _ptr(frhs1), dt, order or self.rkmts,
-                                          self._prec(precision)))
+        nb = int(np.prod(f.shape)) // self.N
+        if nb == 1:
+            self._check(self._lib.dgv_step_rk(self._h, _ptr(f), _ptr(frhs1), dt, order or self.rkmts,
+                                              self._prec(precision)))
+        else:
+            self._check(self._lib.dgv_step_rk_batched(self._h, nb, _ptr(f), _ptr(frhs1), dt, order or self.rkmts,
+                                                      self._prec(precision)))
         return frhs1
 
     def PrepareMTS_SH_DGV(self, f, dt, order=None, precision=None):

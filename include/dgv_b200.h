@@ -65,6 +65,13 @@ extern "C" {
 #define DGV_OPT_TCSETMB 6  /* block form: MB of block records per kernel     */
                            /* launch (default 48; a launch's records are read */
                            /* by all its CTAs, so they should stay in L2)     */
+#define DGV_OPT_WAIT_LIMIT_US 7  /* block form: microseconds after which a    */
+                                 /* bounded device wait gives up (0 = 4 s);   */
+                                 /* the call then returns DGV_ETIMEOUT        */
+#define DGV_OPT_TEST_WITHHOLD 8  /* 1: test of the bounded waits: the next    */
+                                 /* block-form call leaves one of its copies  */
+                                 /* unissued, so its waits run out and it     */
+                                 /* returns DGV_ETIMEOUT; resets itself       */
 
 typedef struct dgv_ctx dgv_ctx;
 
@@ -240,6 +247,14 @@ int dgv_collide_f64_noalloc(dgv_ctx *ctx, const double *f, double *q, int32_t nb
  * receives the first-stage right side divided by dt, as the reference leaves
  * it in commvar's frhs1. */
 int dgv_step_rk(dgv_ctx *ctx, double *f, double *frhs1, double dt, int order, int precision);
+/* One RK step of order 1..5 for nb VDFs stored contiguously (f[nb][N], in
+ * place; frhs1 [nb][N] or NULL): TimeIntegratorORK_SH_DGV
+ * (time_integr_mod.f90:26-152) applied to every VDF, with each stage's Q of
+ * the whole batch evaluated in one call (the tensor-core path evaluates it
+ * in one pass); captured into a CUDA graph from the second call with the
+ * same arrays, as dgv_step_rk.  Run modes (dgv_set_regime) are per VDF:
+ * with them on, nb > 1 gives DGV_EUNSUP. */
+int dgv_step_rk_batched(dgv_ctx *ctx, int32_t nb, double *f, double *frhs1, double dt, int order, int precision);
 /* Adams-Bashforth start-up: order-1 RK steps of that order, filling the
  * right-side history kept in the context (PrepareMTS_SH_DGV, time_integr_mod.f90:443-569). */
 int dgv_prepare_ab(dgv_ctx *ctx, double *f, double dt, int order, int precision);

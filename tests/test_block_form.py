@@ -106,13 +106,15 @@ def test_block_form_adjoint_equals_oracle_vjp(s, M, L, seed):
 def test_adjoint_kernel_schedule_equals_oracle_vjp(s, M, L, seed):
     """The schedule of the tensor-core adjoint kernel, restated: a CTA owns a
     target cell T; each block (c1 <= c2) gives two items per valid output
-    cell D of its box (the per-axis bounds of the device layout):
+    cell D of its box (the per-axis bounds of the device layout), each with
+    records compacted to one of the block's node masks:
       pass 1: T = D + (c1 - cc) (linear indices), side = c(D), operand
-              f(D + c2 - cc), records W1[n = p*P + l1, k = l2];
+              f(D + c2 - cc), records W[n = rank(l1)*P + p, k = l2] (the
+              collision operator's own), mask of the nodes l1;
       pass 2: T = D + (c2 - cc), side = c(D), operand f(D + c1 - cc),
-              records W2[n = p*P + l2, k = l1];
-    and per row acc[n % P] += side[n / P] * (f W^T)[n], added to g(T).
-    Equals the oracle's VJP to 1e-13."""
+              records W2[n = rank(l2)*P + p, k = l1], mask of the nodes l2;
+    per row, node l of the mask gets sum_p side[p] * (f W^T)[rank(l)*P + p],
+    added to g(T, l).  Equals the oracle's VJP to 1e-13."""
     from oracle.oracle import Oracle
     o = Oracle(s, M, L)
     cap, A, xi, xi1 = o.synth_A(seed=seed, support=1)
@@ -131,6 +133,7 @@ def test_adjoint_kernel_schedule_equals_oracle_vjp(s, M, L, seed):
     cq = (2.0 * v / o.gwts).reshape(Nc, P)
     c3 = _cell3(np.array(cc), M)
     g = np.zeros((Nc, P))
+    partial = 0
     for (a, b), W in blocks.items():
         assert a <= b
         e1, e2 = _cell3(np.array(a), M), _cell3(np.array(b), M)
@@ -138,18 +141,20 @@ def test_adjoint_kernel_schedule_equals_oracle_vjp(s, M, L, seed):
         hi = np.minimum(M - 1, c3 + M - 1 - np.maximum(e1, e2))
         if np.any(hi < lo):
             continue
-        W1 = W.transpose(2, 1, 0).reshape(P * P, P)   # [n = p*P + l1, k = l2]
-        W2 = W.transpose(2, 0, 1).reshape(P * P, P)   # [n = p*P + l2, k = l1]
+        present = W.any(axis=2)                       # [l2, l1]
+        m1, m2 = np.nonzero(present.any(axis=0))[0], np.nonzero(present.any(axis=1))[0]
+        partial += (len(m1) < P) + (len(m2) < P)
+        W1 = W[:, m1, :].transpose(1, 2, 0).reshape(len(m1) * P, P)   # [rank(l1)*P + p, l2]
+        W2 = W[m2, :, :].transpose(0, 2, 1).reshape(len(m2) * P, P)   # [rank(l2)*P + p, l1]
         o1, o2 = a - cc, b - cc
         for u in range(lo[0], hi[0] + 1):
             for vv in range(lo[1], hi[1] + 1):
                 for w in range(lo[2], hi[2] + 1):
                     D = (u * M + vv) * M + w
-                    for T, opnd, Wr in ((D + o1, D + o2, W1), (D + o2, D + o1, W2)):
-                        G = Wr @ fc[opnd]                      # [n]
-                        acc = np.zeros(P)
-                        for n in range(P * P):
-                            acc[n % P] += cq[D, n // P] * G[n]
-                        g[T] += acc
+                    for T, opnd, Wr, nodes in ((D + o1, D + o2, W1, m1), (D + o2, D + o1, W2, m2)):
+                        G = (Wr @ fc[opnd]).reshape(len(nodes), P)  # [rank, p]
+                        for r, l in enumerate(nodes):
+                            g[T, l] += cq[D] @ G[r]
     ref = o.vjp(f, v)
+    assert partial > 0  # some blocks use only part of their nodes
     assert np.linalg.norm(g.ravel() - ref) / np.linalg.norm(ref) < 1e-13
