@@ -2,9 +2,9 @@
 
 ``collision(f, solver)`` is Q(f,f) (``EvalCollisionPeriodicAPlus_DGV``,
 collision_mod.f90:143-229) as a differentiable torch op: its backward is the
-library's vector-Jacobian product (``dgv_vjp``, the adjoint of
-collision_mod.f90:213-216), evaluated in FP64 whatever precision the forward
-used.  ``rk_step`` is one step of ``TimeIntegratorORK_SH_DGV``
+library's vector-Jacobian product (the adjoint of collision_mod.f90:213-216):
+for a forward on the tensor cores the batched tensor-core VJP
+(``dgv_vjp_batched``), otherwise the FP64 VJP.  ``rk_step`` is one step of ``TimeIntegratorORK_SH_DGV``
 (time_integr_mod.f90:26-152) with the reference's stage coefficients; its
 backward is the discrete adjoint of the step.  Only the step's input is kept
 (a checkpoint); the backward recomputes the stages and walks them in reverse,
@@ -12,7 +12,7 @@ one VJP per stage.  ``rk_trajectory`` chains steps, so memory grows with the
 number of steps by one state each.
 
 The solver argument needs ``collide(f, out, precision=)``, ``vjp(f, v, out)``
-and ``kappa``; a ``DGVSolver`` (device tensors, used in place) is the
+(with ``precision=`` for the tensor-core backward) and ``kappa``; a ``DGVSolver`` (device tensors, used in place) is the
 intended one.  The FP64 conservation projection has no adjoint here: the
 wrappers refuse a solver with the projection switched on.
 """
@@ -61,14 +61,19 @@ def _q(solver, f, scale, precision):
     return q * scale if scale != 1.0 else q
 
 
-def _vjp(solver, f, v, scale):
-    """scale * J(f)^T v, row by row for a batch"""
+def _vjp(solver, f, v, scale, precision="f64"):
+    """scale * J(f)^T v: the whole batch in one tensor-core call when the
+    forward ran on the tensor cores (dgv_vjp_batched, DGV_PREC_TC), else the
+    FP64 VJP row by row"""
     fr, vr = _rows(f.contiguous()), _rows(v.contiguous())
     g = torch.empty_like(fr)
     _sync(fr)
     _sync(vr)
-    for b in range(fr.shape[0]):
-        solver.vjp(fr[b].contiguous(), vr[b].contiguous(), g[b])
+    if precision == "tc":
+        solver.vjp(fr, vr, g, precision="tc")
+    else:
+        for b in range(fr.shape[0]):
+            solver.vjp(fr[b].contiguous(), vr[b].contiguous(), g[b])
     g = g.reshape(f.shape)
     return g * scale if scale != 1.0 else g
 
@@ -76,14 +81,14 @@ def _vjp(solver, f, v, scale):
 class _Collision(torch.autograd.Function):
     @staticmethod
     def forward(ctx, f, solver, scale, precision):
-        ctx.solver, ctx.scale = solver, scale
+        ctx.solver, ctx.scale, ctx.precision = solver, scale, precision
         ctx.save_for_backward(f)
         return _q(solver, f, scale, precision)
 
     @staticmethod
     def backward(ctx, gq):
         (f,) = ctx.saved_tensors
-        return _vjp(ctx.solver, f, gq, ctx.scale), None, None, None
+        return _vjp(ctx.solver, f, gq, ctx.scale, ctx.precision), None, None, None
 
 
 def collision(f: torch.Tensor, solver, scale: float = 1.0, precision: str = "f64") -> torch.Tensor:
@@ -136,7 +141,7 @@ class _RKStep(torch.autograd.Function):
             for m in range(i + 1, ns):
                 if i < len(A[m]) and A[m][i] != 0.0:
                     k_bar = k_bar + A[m][i] * s_bar[m]
-            s_bar[i] = _vjp(solver, s_list[i], k_bar, h)
+            s_bar[i] = _vjp(solver, s_list[i], k_bar, h, ctx.precision)
             gf = gf + s_bar[i]
         return gf, None, None, None, None
 

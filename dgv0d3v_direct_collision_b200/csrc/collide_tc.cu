@@ -107,6 +107,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
 // registers written by the tcgen05.ld forms below are valid after tmem_wait_ld()
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// the same wait with the 32 registers of one load as operands: no use of them
+// can be scheduled before it
+__device__ __forceinline__ void tmem_wait_ld32(uint32_t *r)
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]),
+                   "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                   "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
+
 // 32 consecutive columns of this warp's lane quarter in one instruction (no wait)
 __device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t *r)
 {
@@ -794,9 +807,9 @@ constexpr int T2_NSTW = 3;                    // W ring stages
 constexpr int T2_ATILE = TC_ROWS * T2_K * 2;  // 128 rows x 32 fp16 (8 KiB)
 constexpr int T2_EPI_WARPS = 8;
 // slot header, after the side tile of the slot's first VDF tile: the item's
-// column count and, for each rank jj of its mask, the offset (floats) l*VB of
-// the node l in the side tile (-1 past the mask's nodes); written by the
-// producer before it arms the slot
+// column count, for each rank jj of its mask the offset (floats) l*VB of the
+// node l in the side tile (-1 past the mask's nodes), and the item's nch;
+// written by the producer before it arms the slot
 constexpr int T2_HDR = 128;
 constexpr int T2_THREADS = 32 * (2 + T2_EPI_WARPS);
 
@@ -978,10 +991,17 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // zero the item slots once: the copies of an item skip cells outside the
+    // grid, so rows of such cells read what the slot held before -- zeros or
+    // finite values of earlier items, which the zero side factors of rows an
+    // item does not serve turn into exact zeros
+    for (int t = threadIdx.x; t < a.region / 4; t += blockDim.x)
+        reinterpret_cast<uint4 *>(slots)[t] = make_uint4(0u, 0u, 0u, 0u);
+    fence_async_shared();  // visible to the tensor core and ordered before the copies
     if (warp >= 2) {
         // zero all 512 columns once (warps 2-5 the first 256, 6-9 the rest, each
         // its lane quarter): an item's last column group may be narrower than
-        // the 64-column loads of the epilogue, whose extra columns then hold
+        // the 32-column loads of the epilogue, whose extra columns then hold
         // zeros or finite values of earlier jobs, times a zero factor
         const float z[16] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         const uint32_t tq = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(((warp - 2) >> 2) * 256);
@@ -1016,6 +1036,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                         if ((msk >> l) & 1u) hd[1 + k++] = l * VB;
                     hd[0] = k * P;
                     for (; k < P; k++) hd[1 + k] = -1;
+                    hd[1 + P] = e.nch;
                 }
                 uint32_t tx = 0;
                 if (hi1 > lo1) tx += (uint32_t)(nb2 * (hi1 - lo1) * P * VB * 4);
@@ -1120,36 +1141,48 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
 #pragma unroll
         for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
         int q = 0, gq = 0;  // items and column groups consumed so far
+        float acc[MODE == 0 ? P : 1];  // MODE 0: the open items' FP32 sums
+        int nacc = 0;                  // items in acc
+#pragma unroll
+        for (int p = 0; p < (MODE == 0 ? P : 1); p++) acc[p] = 0.f;
         bool ok = true;
         for (int it = i0; it < i1 && ok; it++) {
-            const int nch = a.items[it].nch;
-            const bool valid = (nch >> (27 + d)) & 1;
-            const unsigned msk = (unsigned)nch & 0x7ffffffu;
-            const int nl = __popc(msk), ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
             const int s = q & 1;
             if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
             const float *f1s =
                 reinterpret_cast<const float *>(slots + (size_t)(2 * s + j) * a.region + 2 * T2_ATILE) + d * P * VB + v;
             const int *hoff =
                 reinterpret_cast<const int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE + NDG * P * VB * 4) + 1;
+            const int nch = hoff[P];
+            const bool valid = (nch >> (27 + d)) & 1;
+            const unsigned msk = (unsigned)nch & 0x7ffffffu;
+            const int nl = __popc(msk), ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
             // Columns n = jj*P + p, jj = the rank of a node of the item's mask.
             // MODE 0: side = f(c1 + D, l1) of the jj-th node l1 (its offset from
-            //         the slot header), loaded at its first column (all 27 live
-            //         at once would spill), acc[p] += side * G[n].
+            //         the slot header; 0 past the mask's nodes),
+            //         acc[p] += side * G[n].
             // MODE 1: side = c(D, p) (all P live), the sum over p of each jj is
             //         complete after its P consecutive columns and is kept in
             //         stg[jj] (local memory: its read index is the rank of a
             //         node); after the item each node l of the mask adds
             //         stg[rank(l)] into its (sum, correction).
-            float f1[MODE == 1 ? P : 1], acc[MODE == 0 ? P : 1], stg[MODE == 1 ? P : 1], fcur = 0.f, run = 0.f;
+            float f1[P], stg[MODE == 1 ? P : 1], run[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int l = 0; l < P; l++) {
-                if constexpr (MODE == 1) f1[l] = f1s[l * VB];
-                else acc[l] = 0.f;
+                if constexpr (MODE == 1) {
+                    f1[l] = f1s[l * VB];
+                } else {
+                    // loaded before the column loop (the TMEM waits order all
+                    // shared-memory loads, so loads inside it would stall); a
+                    // row the item does not serve gets zero factors, so its
+                    // columns add exact zeros
+                    const int o = hoff[l];
+                    f1[l] = (valid && o >= 0) ? f1s[o] : 0.f;
+                }
             }
-            // MODE 0: two 32-column loads per wait (the load latency is paid four
-            // times per 256-column group); MODE 1 keeps more values live: one
-            constexpr int LW = MODE == 0 ? 64 : 32;
+            // one 32-column load per wait (two per wait, with the side factors
+            // and sums live, would spill)
+            constexpr int LW = 32;
 #pragma unroll
             for (int g = 0; g < NG; g++) {
                 if (g >= ngb) break;
@@ -1161,29 +1194,19 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                     if (g * T2_N + LW * hh >= P * P || g * T2_N + LW * hh >= ncol) break;
                     uint32_t G[LW];
                     tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + LW * hh), G);
-                    if (LW == 64 && g * T2_N + LW * hh + 32 < P * P) {
-                        if (g * T2_N + LW * hh + 32 < ncol) {
-                            tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + LW * hh + 32), G + 32);
-                        } else {
-#pragma unroll
-                            for (int i = 32; i < LW; i++) G[i] = 0u;
-                        }
-                    }
-                    tmem_wait_ld();
+                    tmem_wait_ld32(G);
 #pragma unroll
                     for (int i = 0; i < LW; i++) {
                         const int n = g * T2_N + LW * hh + i;
                         if (n < P * P) {
                             if constexpr (MODE == 0) {
-                                if (n % P == 0 || i == 0) {
-                                    const int o = hoff[n / P];
-                                    fcur = o >= 0 ? f1s[o] : 0.f;
-                                }
-                                acc[n % P] = fmaf(fcur, __uint_as_float(G[i]), acc[n % P]);
+                                acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
                             } else {
-                                run = n % P == 0 ? f1[0] * __uint_as_float(G[i])
-                                                 : fmaf(f1[n % P], __uint_as_float(G[i]), run);
-                                if (n % P == P - 1) stg[n / P] = run;
+                                // three interleaved partial sums over p
+                                const int pp = n % P, r = pp % 3;
+                                run[r] = pp < 3 ? f1[pp] * __uint_as_float(G[i])
+                                                : fmaf(f1[pp], __uint_as_float(G[i]), run[r]);
+                                if (pp == P - 1) stg[n / P] = (run[0] + run[1]) + run[2];
                             }
                         }
                     }
@@ -1196,22 +1219,40 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             gq += ngb;
             __syncwarp();
             if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
-            if (valid) {
+            if constexpr (MODE == 0) {
+                // two items' totals summed in FP32, then two-summed into (sum,
+                // correction)
+                if (++nacc == 2) {
 #pragma unroll
-                for (int p = 0; p < P; p++) {  // two-sum of the block total into (sum, correction)
-                    float x;
-                    if constexpr (MODE == 0) {
-                        x = acc[p];
-                    } else {
-                        if (!((msk >> p) & 1u)) continue;
-                        x = stg[__popc(msk & ((1u << p) - 1u))];
+                    for (int p = 0; p < P; p++) {
+                        const float t = S[p] + acc[p], bpv = t - S[p];
+                        Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
+                        S[p] = t;
+                        acc[p] = 0.f;
                     }
+                    nacc = 0;
+                }
+            } else if (valid) {
+#pragma unroll
+                for (int p = 0; p < P; p++) {  // two-sum of the node totals into (sum, correction)
+                    if (!((msk >> p) & 1u)) continue;
+                    const float x = stg[__popc(msk & ((1u << p) - 1u))];
                     const float t = S[p] + x, bpv = t - S[p];
                     Cc[p] += (S[p] - (t - bpv)) + (x - bpv);
                     S[p] = t;
                 }
             }
             q++;
+        }
+        if constexpr (MODE == 0) {
+            if (ok && nacc) {
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const float t = S[p] + acc[p], bpv = t - S[p];
+                    Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
+                    S[p] = t;
+                }
+            }
         }
         if (ok) {
             const int D = D0 + d, vdf = (bt0 + j) * VB + v;

@@ -40,7 +40,10 @@ def test_batched_and_tensor_core_forward(gsol, golden):
     assert rel_err(q[0].detach().cpu().numpy(), golden["q0"]) < 1e-6
     q.sum().backward()
     g = f.grad.cpu().numpy()
-    assert rel_err(g[1], 0.5 * g[0]) < 1e-12  # J(f) is linear in f
+    assert rel_err(g[1], 0.5 * g[0]) < 1e-12  # J(f) is linear in f (and the scaling exact)
+    # the tensor-core forward's backward is the tensor-core VJP of the batch
+    o = golden_oracle(golden)
+    assert rel_err(g[0], o.vjp(golden["f0"], np.ones(o.N))) < 1e-6
 
 
 @pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
