@@ -147,22 +147,37 @@ def balanced_cells(Mc: int):
     return np.random.default_rng(0).permutation(np.array(cells))
 
 
+def synth_A_some(o, ps):
+    """The oracle's synthetic records of the basis functions ps only (the
+    records of one basis function are only read by the nodes of that basis
+    function, collision_mod.f90:186-188), in the reference layout."""
+    parts = {p: o.synth_A(seed=SEED_A, support=1, p_only=p) for p in ps}
+    cap = np.sum([q[0] for q in parts.values()], axis=0).astype(np.int32)
+    ordered = [parts[p] for p in sorted(ps)]  # records in node order
+    A = np.concatenate([q[1] for q in ordered])
+    xi = np.concatenate([q[2] for q in ordered])
+    xi1 = np.concatenate([q[3] for q in ordered])
+    return cap, A, xi, xi1
+
+
 class CpuBaseline:
     """Oracle (CPU restatement of EvalCollisionPeriodicAPlus_DGV) on a sample
-    of output nodes of the same workload.  All nodes scan the same record
-    list (the records of their canonical basis function), so time per node x
-    N gives the time of one full evaluation.  Set up once (grid, synthetic A
-    of basis function 13, f), then timed as often as asked."""
-    P_SAMPLE = 13
+    of output nodes of the same workload.  All nodes of one basis function
+    scan the same record list, so time per node x N gives the time of one
+    full evaluation.  The sample: the balanced cells of the grid at three
+    basis functions (243 nodes at 27^3, ~15 rounds of 16 threads, so the
+    threads idle at the end of the last round matter little).  Set up once
+    (grid, synthetic A of those basis functions, f), then timed as often as
+    asked."""
+    P_SAMPLE = (4, 13, 22)
 
     def __init__(self, nthreads: int = 0):
         from oracle.oracle import Oracle
         self.o = Oracle(S, M, L)
-        cap, A, xi, xi1 = self.o.synth_A(seed=SEED_A, support=1, p_only=self.P_SAMPLE)
-        self.o.set_A(cap, A, xi, xi1)
+        self.o.set_A(*synth_A_some(self.o, self.P_SAMPLE))
         self.f = mixture_batch(self.o.u, self.o.v, self.o.w, self.o.gwts, 1, 7)[0]
         self.cores = nthreads or os.cpu_count()
-        self.nodes_all = balanced_cells(M) * self.o.P + self.P_SAMPLE
+        self.nodes_all = np.array([c * self.o.P + p for c in balanced_cells(M) for p in self.P_SAMPLE])
         self.n = None
 
     def sample(self, seconds_target: float = 15.0):
@@ -182,17 +197,17 @@ class CpuBaseline:
         dt1 = time.perf_counter() - t
         eval_s = dt1 / self.n * o.N
         return {"value": 1.0 / eval_s, "unit": "evals/s", "cores": self.cores, "kind": "port",
-                "sample": f"{self.n} of {o.N} output nodes of one 27^3 VDF (records of basis function "
-                          f"{self.P_SAMPLE}, cells of a balanced sample of {nall}), {dt1:.1f} s; full evaluation "
-                          f"= time per node x N"}, dt1
+                "sample": f"{self.n} of {o.N} output nodes of one 27^3 VDF (basis functions "
+                          f"{list(self.P_SAMPLE)} at the {len(balanced_cells(M))} balanced cells), {dt1:.1f} s; "
+                          f"full evaluation = time per node x N"}, dt1
 
 
 def calibrate_sampling(nthreads: int = 0):
     """Checks the node-sample estimate against a full evaluation where one is
     cheap: the 15^3 grid (s=3, M=5, [-6,6]^3, all 27 basis functions' synthetic
     records), one seeded mixture VDF.  The full oracle evaluation is timed once,
-    and the estimate the 27^3 baseline uses (records of basis function 13 only,
-    a node sample of that basis function, time per node x N) beside it."""
+    and the estimate the 27^3 baseline uses (balanced cells, whole rounds of
+    the threads, time per node x N) beside it."""
     from oracle.oracle import Oracle
     cores = nthreads or os.cpu_count()
     o = Oracle(3, 5, 6.0)
@@ -202,8 +217,9 @@ def calibrate_sampling(nthreads: int = 0):
     o.collide(f, nthreads=cores)
     full = time.perf_counter() - t
     # the estimator of the 27^3 baseline: balanced cells, whole rounds of the
-    # threads, time per node x N (three basis functions here, for enough nodes)
-    cand = np.array([c * o.P + p for c in balanced_cells(5) for p in (CpuBaseline.P_SAMPLE, 4, 22)])
+    # threads, time per node x N (nine basis functions here: 225 nodes, about
+    # as many rounds as the 27^3 sample)
+    cand = np.array([c * o.P + p for c in balanced_cells(5) for p in range(0, o.P, 3)])
     nodes = cand[:max(cores, len(cand) // cores * cores)]
     t = time.perf_counter()
     o.collide(f, nodes=nodes, nthreads=cores)

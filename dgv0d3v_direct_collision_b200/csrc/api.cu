@@ -334,11 +334,13 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
     case DGV_OPT_TCSETMB:
         if (value < 1 || value > 4096) return set_err(&ctx->c, DGV_EINVAL, "records per launch must be 1..4096 MB");
         ctx->c.tc_set_mb = (int)value;
+        ctx->c.tc_user_launch = true;
         release_graphs(&ctx->c);
         return DGV_OK;
     case DGV_OPT_TCTILES:
         if (value != 1 && value != 2) return set_err(&ctx->c, DGV_EINVAL, "VDF tiles per CTA must be 1 or 2");
         ctx->c.tc_tiles_per_cta = (int)value;
+        ctx->c.tc_user_launch = true;
         release_graphs(&ctx->c);
         return DGV_OK;
     case DGV_OPT_TCFORM:
@@ -353,6 +355,17 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
         return DGV_OK;
     case DGV_OPT_TEST_WITHHOLD:
         ctx->c.test_withhold = value != 0;
+        return DGV_OK;
+    case DGV_OPT_TCAUTOTUNE:
+        ctx->c.tc_autotune = value != 0;
+        if (!value) {  // back to the fixed defaults (unless the caller set them)
+            ctx->c.tc_tuned.clear();
+            if (!ctx->c.tc_user_launch) {
+                ctx->c.tc_tiles_per_cta = 2;
+                ctx->c.tc_set_mb = 48;
+            }
+        }
+        release_graphs(&ctx->c);
         return DGV_OK;
     default: return set_err(&ctx->c, DGV_EINVAL, "unknown option");
     }

@@ -1141,8 +1141,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
 #pragma unroll
         for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
         int q = 0, gq = 0;  // items and column groups consumed so far
-        float acc[MODE == 0 ? P : 1];  // MODE 0: the open items' FP32 sums
-        int nacc = 0;                  // items in acc
+        float acc[MODE == 0 ? P : 1];  // MODE 0: the item's FP32 sums
 #pragma unroll
         for (int p = 0; p < (MODE == 0 ? P : 1); p++) acc[p] = 0.f;
         bool ok = true;
@@ -1220,17 +1219,14 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             __syncwarp();
             if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
             if constexpr (MODE == 0) {
-                // two items' totals summed in FP32, then two-summed into (sum,
-                // correction)
-                if (++nacc == 2) {
+                // the item's total two-summed into (sum, correction); a row the
+                // item does not serve adds exact zeros (zero side factors)
 #pragma unroll
-                    for (int p = 0; p < P; p++) {
-                        const float t = S[p] + acc[p], bpv = t - S[p];
-                        Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
-                        S[p] = t;
-                        acc[p] = 0.f;
-                    }
-                    nacc = 0;
+                for (int p = 0; p < P; p++) {
+                    const float t = S[p] + acc[p], bpv = t - S[p];
+                    Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
+                    S[p] = t;
+                    acc[p] = 0.f;
                 }
             } else if (valid) {
 #pragma unroll
@@ -1243,16 +1239,6 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                 }
             }
             q++;
-        }
-        if constexpr (MODE == 0) {
-            if (ok && nacc) {
-#pragma unroll
-                for (int p = 0; p < P; p++) {
-                    const float t = S[p] + acc[p], bpv = t - S[p];
-                    Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
-                    S[p] = t;
-                }
-            }
         }
         if (ok) {
             const int D = D0 + d, vdf = (bt0 + j) * VB + v;
@@ -1393,7 +1379,7 @@ static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, int VB)
     }
 }
 
-static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
+static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
@@ -1441,6 +1427,74 @@ static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, 
     count_launches(c, 3);  // k_tc_fprep, k_tc2_f16, k_tc_final
     if (c->project) return project_device(c, d_q, nvdf);
     return DGV_OK;
+}
+
+// The block form's launch choices, tuned on the first evaluation of each
+// batch class (VDF tile size; one or several VDF tiles): VDF tiles per CTA (two
+// let a block's records cross from L2 once per 256 rows, one gives twice the
+// CTAs) and block records per launch (the records one launch streams should
+// stay in L2 while all its CTAs read them).  Each candidate is evaluated once to
+// warm up (work lists) and once timed with CUDA events on the context stream;
+// the fastest is kept for the context.  Not while the stream is being captured
+// (the current choice serves), and not when the caller set either option.
+static int tc2_autotune(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
+{
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32);
+    const int nbt = (nvdf + VB - 1) / VB;
+    const int key = VB * 2 + (nbt > 1 ? 1 : 0);
+    auto it = c->tc_tuned.find(key);
+    if (it != c->tc_tuned.end()) {
+        c->tc_tiles_per_cta = it->second.first;
+        c->tc_set_mb = it->second.second;
+        return DGV_OK;
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    DGV_CUDA(c, cudaStreamIsCapturing(c->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return DGV_OK;
+    const bool kt = c->ktiming;
+    const long long kt_all = c->kt_all;
+    c->ktiming = false;
+    const int tiles[2] = {2, 1}, mbs[3] = {24, 48, 96};
+    float best_ms = 1e30f;
+    int best_t = c->tc_tiles_per_cta, best_mb = c->tc_set_mb, rc = DGV_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DGV_CUDA(c, cudaEventCreate(&e0));
+    DGV_CUDA(c, cudaEventCreate(&e1));
+    for (int t : tiles) {
+        if (t > 1 && nbt < 2) continue;
+        for (int mb : mbs) {
+            c->tc_tiles_per_cta = t;
+            c->tc_set_mb = mb;
+            if ((rc = collide_tc2_body(c, d_f, d_q, nvdf, scale))) break;
+            cudaEventRecord(e0, c->stream);
+            if ((rc = collide_tc2_body(c, d_f, d_q, nvdf, scale))) break;
+            cudaEventRecord(e1, c->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) { rc = set_err(c, DGV_ECUDA, "autotune: event failed"); break; }
+            if ((rc = check_errflag(c))) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) { best_ms = ms; best_t = t; best_mb = mb; }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->ktiming = kt;
+    c->kt_all = kt_all;
+    c->tc_tiles_per_cta = best_t;
+    c->tc_set_mb = best_mb;
+    if (rc) return rc;
+    c->tc_tuned[key] = {best_t, best_mb};
+    return DGV_OK;
+}
+
+static int collide_tc2_device(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
+{
+    if (c->tc_autotune && !c->tc_user_launch) {
+        const int rc = tc2_autotune(c, d_f, d_q, nvdf, scale);
+        if (rc) return rc;
+    }
+    return collide_tc2_body(c, d_f, d_q, nvdf, scale);
 }
 
 // ----------------------------------------------------------------------------
@@ -1635,6 +1689,13 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
         block = false;  // as collide_tc_device: the chunk form serves
     }
     if (block) {
+        if (c->tc_autotune && !c->tc_user_launch) {  // the choice tuned for this batch class, if any
+            auto it = c->tc_tuned.find(VB * 2 + (nbt > 1 ? 1 : 0));
+            if (it != c->tc_tuned.end()) {
+                c->tc_tiles_per_cta = it->second.first;
+                c->tc_set_mb = it->second.second;
+            }
+        }
         tc2_sets(c);
         std::vector<int> first, count;
         if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl, 1))) return rc;

@@ -143,6 +143,9 @@ struct Ctx {
     int tc_tiles_per_cta = 2;  // DGV_OPT_TCTILES: VDF tiles per CTA in the block form
     int tc_set_mb = 48;        // DGV_OPT_TCSETMB: block form, MB of records per launch
     long long wait_limit_us = 0;  // DGV_OPT_WAIT_LIMIT_US: bounded waits of the block form (0 = 4 s)
+    bool tc_autotune = true;      // DGV_OPT_TCAUTOTUNE: tune tiles per CTA and records per launch
+    bool tc_user_launch = false;  // the caller set DGV_OPT_TCTILES or DGV_OPT_TCSETMB: no tuning
+    std::map<int, std::pair<int, int>> tc_tuned;  // per batch class: (tiles per CTA, MB per launch)
     bool test_withhold = false;   // DGV_OPT_TEST_WITHHOLD: the next block-form launch withholds one copy
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
     long long kt_launches = 0, kt_all = 0;

@@ -68,6 +68,12 @@ extern "C" {
 #define DGV_OPT_WAIT_LIMIT_US 7  /* block form: microseconds after which a    */
                                  /* bounded device wait gives up (0 = 4 s);   */
                                  /* the call then returns DGV_ETIMEOUT        */
+#define DGV_OPT_TCAUTOTUNE 9      /* block form: 1 (default) = on the first    */
+                                 /* evaluation of each batch class, time VDF  */
+                                 /* tiles per CTA x records per launch and    */
+                                 /* keep the fastest; 0 = the options' values */
+                                 /* (setting DGV_OPT_TCTILES or _TCSETMB also */
+                                 /* switches the tuning off)                  */
 #define DGV_OPT_TEST_WITHHOLD 8  /* 1: test of the bounded waits: the next    */
                                  /* block-form call leaves one of its copies  */
                                  /* unissued, so its waits run out and it     */

@@ -9,8 +9,9 @@ tests of the batched RK steps.  Test infrastructure: runs the oracle only.
       dt = 0.01 for 100 steps; f after steps 1, 10, 50 and 100 and Q(f0).
   c2: the 21^3 grid (s=3, M=7, [-6,6]^3), synthetic A (seed 20260101,
       support 1), kappa = 0.1, f0 = the seeded 1-4 Maxwellian mixture of
-      the benchmark's generator (seed 5); RK4 with dt = 0.005, one step
-      (a full oracle evaluation at 21^3 takes ~10 minutes on 8 cores).
+      the benchmark's generator (seed 5); RK4 with dt = 0.005, 5 steps (a
+      full oracle evaluation at 21^3 takes ~2 minutes on 8 cores); f after
+      steps 1 and 5.
 
 Usage: python tests/golden/make_rk_trajectory.py c1|c2  (writes
 tests/golden/rk_<case>.npz)."""
@@ -49,7 +50,7 @@ def main(case):
         o = Oracle(*grid)
         f = o.maxwellian(1.0, 1.5, 0.0, 0.0, 0.5) + o.maxwellian(1.0, -1.5, 0.0, 0.0, 0.5)
     else:
-        grid, seed_a, kappa, dt, order, steps, keep = (3, 7, 6.0), 20260101, 0.1, 0.005, 4, 1, (1,)
+        grid, seed_a, kappa, dt, order, steps, keep = (3, 7, 6.0), 20260101, 0.1, 0.005, 4, 5, (1, 5)
         o = Oracle(*grid)
         f = mixture(o, 5)
     o.set_A(*o.synth_A(seed=seed_a, support=1))

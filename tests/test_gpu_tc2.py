@@ -112,6 +112,7 @@ def test_tc_plan_matches_launches(c1):
     (dense tiles, three split products)."""
     o, s = c1["oracle"], c1["solver"]
     fs = np.stack([o.maxwellian(1.0, 0.3 * k, 0, 0, 0.8) for k in range(40)])
+    s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")  # settles the tuned launch choice
     plan = s.tc_plan(40)
     s.set_kernel_timing(True)
     s.kernel_stats(reset=True)
@@ -138,3 +139,23 @@ def test_tc2_launch_size_option(c1):
         s.set_tc_set_mb(48)
     assert n8 > n48
     assert rel_err(q8, q48) < 1e-10  # only the grouping of compensated partial sums differs
+
+
+def test_tc2_autotuned_launch_choice():
+    """The first evaluation of a batch class times VDF tiles per CTA x records
+    per launch and keeps the fastest; the results equal those of the fixed
+    default choice (only the grouping of compensated partial sums differs)."""
+    import dgv0d3v_direct_collision_b200 as m
+    from dgv0d3v_direct_collision_b200 import _lib
+    s = m.DGVSolver(3, 5, 6.0)
+    s.generate_synthetic_A(seed=11, support=1)
+    rng = np.random.default_rng(23)
+    fs = np.stack([mixture_vdf(s.nodes_u, s.nodes_v, s.nodes_w, rng, normalise_w=s.nodes_gwts) for _ in range(150)])
+    q_tuned = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    q_again = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    assert np.array_equal(q_tuned, q_again)  # the choice is kept: same launches, same sums
+    L = _lib.load()
+    assert L.dgv_set_option(s._h, _lib.DGV_OPT_TCAUTOTUNE, 0) == 0
+    q_fixed = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
+    assert rel_err(q_tuned, q_fixed) < 1e-10
+    s.close()
