@@ -32,10 +32,14 @@ struct VjpArgs {
     int *err;
     long long N;
     int Nc, Mv, Mw, dcta, rowb, nst, sp, off_f, off_hdr, off_bar;
+    int Pt, npsl;  // nodes per cell; slices of PV basis functions (1 unless sliced)
 };
 
 // Same shared-memory row pipeline as the forward kernel (pipeline.cuh).
-template <int PV>
+// SL (sliced, for many nodes per cell): a CTA forms vA over the PV basis
+// functions of its slice only (blockIdx.y % npsl) and scatters that part;
+// the scatters of the slices add up to the full adjoint.
+template <int PV, bool SL = false>
 __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -45,7 +49,9 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
     StageHdr *hdr = reinterpret_cast<StageHdr *>(smem + a.off_hdr);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + a.off_bar);
     uint64_t *empty = full + a.nst;
-    const int slice = blockIdx.y, chunk = blockIdx.z;
+    const int slice = SL ? blockIdx.y / a.npsl : blockIdx.y, chunk = blockIdx.z;
+    const int PT = SL ? a.Pt : PV;                         // nodes per cell
+    const int pofs = SL ? (blockIdx.y % a.npsl) * PV : 0;  // first basis function of the slice
     if (threadIdx.x == 0) {
         for (int s = 0; s < a.nst; s++) {
             mbar_init(&full[s], 1);
@@ -54,7 +60,7 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
         fence_mbar_init();
     }
     for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
-        int cell = (int)(i / PV), l = (int)(i - (long long)cell * PV);
+        int cell = (int)(i / PT), l = (int)(i - (long long)cell * PT);
         f_s[l * a.Nc + cell] = __ldg(a.f + i);
     }
     __syncthreads();
@@ -73,8 +79,8 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
     double cw[PV];
 #pragma unroll
     for (int j = 0; j < PV; j++) {
-        long long i = (long long)D * PV + j;
-        cw[j] = inD ? 2.0 * a.v[i] / a.w[i] : 0.0;
+        long long i = (long long)D * PT + pofs + j;
+        cw[j] = (inD && pofs + j < PT) ? 2.0 * a.v[i] / a.w[i] : 0.0;
     }
     constexpr int RD = ((1 + PV) + 1) / 2 * 2;
     int cur = -1;
@@ -94,19 +100,27 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
             const unsigned char *st = stages + s * stage_bytes;
 #pragma unroll 2
             for (int k = 0; k < h.n; k++) {
-                const double2 *row = reinterpret_cast<const double2 *>(st + (size_t)k * a.rowb);
-                double rv[RD];
-#pragma unroll
-                for (int t = 0; t < RD / 2; t++) {
-                    double2 x = row[t];
-                    rv[2 * t] = x.x;
-                    rv[2 * t + 1] = x.y;
-                }
-                const long long o = __double_as_longlong(rv[0]);
-                const int q1 = (int)(unsigned)(o & 0xffffffffLL) + D, q2 = (int)(o >> 32) + D;
                 double vA = 0.0;
+                long long o;
+                if constexpr (SL) {
+                    const double *rowd = reinterpret_cast<const double *>(st + (size_t)k * a.rowb);
+                    o = __double_as_longlong(rowd[0]);
 #pragma unroll
-                for (int j = 0; j < PV; j++) vA = fma(rv[1 + j], cw[j], vA);
+                    for (int j = 0; j < PV; j++) vA = fma(rowd[1 + pofs + j], cw[j], vA);
+                } else {
+                    const double2 *row = reinterpret_cast<const double2 *>(st + (size_t)k * a.rowb);
+                    double rv[RD];
+#pragma unroll
+                    for (int t = 0; t < RD / 2; t++) {
+                        double2 x = row[t];
+                        rv[2 * t] = x.x;
+                        rv[2 * t + 1] = x.y;
+                    }
+                    o = __double_as_longlong(rv[0]);
+#pragma unroll
+                    for (int j = 0; j < PV; j++) vA = fma(rv[1 + j], cw[j], vA);
+                }
+                const int q1 = (int)(unsigned)(o & 0xffffffffLL) + D, q2 = (int)(o >> 32) + D;
                 atomicAdd(a.g + q1, vA * f_s[q2]);
                 atomicAdd(a.g + q2, vA * f_s[q1]);
             }
@@ -138,8 +152,10 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     case 1: fn = k_vjp_pipe<1>; break;
     case 8: fn = k_vjp_pipe<8>; break;
     case 27: fn = k_vjp_pipe<27>; break;
-    default: return set_err(c, DGV_EUNSUP, "vjp: this build supports 1, 8 or 27 nodes per cell");
+    case 125: fn = k_vjp_pipe<25, true>; break;  // slices of 25 basis functions per CTA
+    default: return set_err(c, DGV_EUNSUP, "vjp: this build supports 1, 8, 27 or 125 nodes per cell");
     }
+    const int npsl = g.P > 27 ? (g.P + 24) / 25 : 1;
     int maxsm = 0, nsm = 148;
     DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     DGV_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
@@ -169,8 +185,8 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     DGV_CUDA(c, cudaMemsetAsync(c->d_glm, 0, sizeof(double) * (size_t)g.N, c->stream));
     a.f = d_f; a.v = d_v; a.w = c->d_nwt; a.g = c->d_glm; a.blk = L.blk; a.rows = (const char *)L.rows64;
     a.bounds = d_bounds; a.err = c->d_err; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.dcta = dcta;
-    a.rowb = rowb; a.nst = nst; a.sp = sp;
-    fn<<<dim3(1, slices, nchunks), 32 + dcta, smem, c->stream>>>(a);
+    a.rowb = rowb; a.nst = nst; a.sp = sp; a.Pt = g.P; a.npsl = npsl;
+    fn<<<dim3(1, slices * npsl, nchunks), 32 + dcta, smem, c->stream>>>(a);
     DGV_CUDA(c, cudaGetLastError());
     k_lm_to_nodes<<<(unsigned)((g.N + 255) / 256), 256, 0, c->stream>>>(c->d_glm, d_g, g.N, g.Nc, g.P);
     DGV_CUDA(c, cudaGetLastError());

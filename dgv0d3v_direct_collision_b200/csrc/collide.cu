@@ -32,6 +32,7 @@
 namespace dgv {
 
 enum CollideMode { MODE_F64 = 0, MODE_F32C = 1, MODE_BILINEAR = 2 };
+constexpr int P_SLICE = 25;  // basis functions per CTA for grids of more than 27 nodes per cell
 
 struct CollideArgs {
     const double *f;        // [nvdf][N]
@@ -46,6 +47,7 @@ struct CollideArgs {
     int cell0, cell1;       // output cells evaluated: [cell0, cell1)
     int nst, sp;            // pipeline stages, pairs per stage
     int off_f, off_hdr, off_bar;  // shared-memory layout (bytes)
+    int Pt, npsl;           // nodes per cell; slices of PV basis functions per cell (1 unless sliced)
 };
 
 // Knuth's branch-free two-sum: s + c carries x exactly
@@ -66,7 +68,12 @@ __device__ __forceinline__ void two_sum_acc(float &s, float &c, float x)
 //                 added to (sum, correction) with two-sum
 //   MODE_BILINEAR acc_p += v_p * (f(a) g(b) + g(a) f(b)), g gathered from
 //                 global memory (the Jacobian-vector product)
-template <int PV, int MODE>
+//
+// SL (sliced, for many nodes per cell, e.g. P = 125): a CTA serves the PV
+// basis functions p in [ps*PV, ps*PV + PV) of its output cells (ps =
+// blockIdx.y % npsl), reading them from the full rows with scalar loads; the
+// node stride is the runtime Pt.
+template <int PV, int MODE, bool SL = false>
 __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
 {
     using T = typename std::conditional<MODE == MODE_F32C, float, double>::type;
@@ -77,7 +84,9 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
     StageHdr *hdr = reinterpret_cast<StageHdr *>(smem + a.off_hdr);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + a.off_bar);
     uint64_t *empty = full + a.nst;
-    const int vdf = blockIdx.x, slice = blockIdx.y, chunk = blockIdx.z;
+    const int vdf = blockIdx.x, slice = SL ? blockIdx.y / a.npsl : blockIdx.y, chunk = blockIdx.z;
+    const int PT = SL ? a.Pt : PV;                    // nodes per cell
+    const int pofs = SL ? (blockIdx.y % a.npsl) * PV : 0;  // first basis function of the slice
     const int nconsumer_warps = a.dcta / 32;
     if (threadIdx.x == 0) {
         for (int s = 0; s < a.nst; s++) {
@@ -88,7 +97,7 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
     }
     const double *f = a.f + (size_t)vdf * a.N;
     for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
-        int cell = (int)(i / PV), l = (int)(i - (long long)cell * PV);
+        int cell = (int)(i / PT), l = (int)(i - (long long)cell * PT);
         f_s[l * a.Nc + cell] = (T)__ldg(f + i);
     }
     __syncthreads();
@@ -154,15 +163,21 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
                         pa = f_s[ow[(k + 1) * rws] + D];
                         pb = f_s[ow[(k + 1) * rws + 1] + D];
                     }
-                    const float4 *row = reinterpret_cast<const float4 *>(st + (size_t)k * a.rowb);
-                    float rv[RW];
+                    if constexpr (SL) {
+                        const float *rowf = reinterpret_cast<const float *>(st + (size_t)k * a.rowb) + 2 + pofs;
 #pragma unroll
-                    for (int t = 0; t < RW / 4; t++) {
-                        float4 x = row[t];
-                        rv[4 * t] = x.x; rv[4 * t + 1] = x.y; rv[4 * t + 2] = x.z; rv[4 * t + 3] = x.w;
+                        for (int j = 0; j < PV; j++) part[j] = fmaf(rowf[j], prod, part[j]);
+                    } else {
+                        const float4 *row = reinterpret_cast<const float4 *>(st + (size_t)k * a.rowb);
+                        float rv[RW];
+#pragma unroll
+                        for (int t = 0; t < RW / 4; t++) {
+                            float4 x = row[t];
+                            rv[4 * t] = x.x; rv[4 * t + 1] = x.y; rv[4 * t + 2] = x.z; rv[4 * t + 3] = x.w;
+                        }
+#pragma unroll
+                        for (int j = 0; j < PV; j++) part[j] = fmaf(rv[2 + j], prod, part[j]);
                     }
-#pragma unroll
-                    for (int j = 0; j < PV; j++) part[j] = fmaf(rv[2 + j], prod, part[j]);
                     if (++npend == 16) {
 #pragma unroll
                         for (int j = 0; j < PV; j++) { two_sum_acc(acc[j], cmp[j], part[j]); part[j] = 0.f; }
@@ -177,8 +192,8 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
                 double ga = 0.0, gb = 0.0;
                 if constexpr (MODE == MODE_BILINEAR) {
                     const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
-                    ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PV + l1);
-                    gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PV + l2);
+                    ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PT + l1);
+                    gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PT + l2);
                 }
                 for (int k = 0; k < h.n; k++) {
                     double prod;
@@ -191,19 +206,25 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
                         pb = f_s[q2];
                         if constexpr (MODE == MODE_BILINEAR) {
                             const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
-                            ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PV + l1);
-                            gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PV + l2);
+                            ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PT + l1);
+                            gb = __ldg(g + (long long)(q2 - l2 * a.Nc) * PT + l2);
                         }
                     }
                     // values v[0..P-1] start at byte 8 of the row; each 16-byte
                     // load is consumed at once to keep few values live
-                    const double2 *row2 = reinterpret_cast<const double2 *>(st + (size_t)k * a.rowb);
-                    acc[0] = fma(row2[0].y, prod, acc[0]);
+                    if constexpr (SL) {
+                        const double *rowd = reinterpret_cast<const double *>(st + (size_t)k * a.rowb) + 1 + pofs;
 #pragma unroll
-                    for (int t = 1; t < RD / 2; t++) {
-                        const double2 x = row2[t];
-                        if (2 * t - 1 < PV) acc[2 * t - 1] = fma(x.x, prod, acc[2 * t - 1]);
-                        if (2 * t < PV) acc[2 * t] = fma(x.y, prod, acc[2 * t]);
+                        for (int j = 0; j < PV; j++) acc[j] = fma(rowd[j], prod, acc[j]);
+                    } else {
+                        const double2 *row2 = reinterpret_cast<const double2 *>(st + (size_t)k * a.rowb);
+                        acc[0] = fma(row2[0].y, prod, acc[0]);
+#pragma unroll
+                        for (int t = 1; t < RD / 2; t++) {
+                            const double2 x = row2[t];
+                            if (2 * t - 1 < PV) acc[2 * t - 1] = fma(x.x, prod, acc[2 * t - 1]);
+                            if (2 * t < PV) acc[2 * t] = fma(x.y, prod, acc[2 * t]);
+                        }
                     }
                 }
             }
@@ -218,12 +239,12 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
         }
     }
     if (inD) {
-        double *out = a.partial + ((size_t)vdf * a.nchunks + chunk) * PV * a.Nc;
+        double *out = a.partial + ((size_t)vdf * a.nchunks + chunk) * PT * a.Nc + (size_t)pofs * a.Nc;
 #pragma unroll
         for (int j = 0; j < PV; j++) {
             double v = (double)acc[j];
             if constexpr (MODE == MODE_F32C) v += (double)cmp[j];
-            out[(size_t)j * a.Nc + D] = v;
+            if (!SL || pofs + j < PT) out[(size_t)j * a.Nc + D] = v;
         }
     }
 }
@@ -263,10 +284,17 @@ static KernelFn pick_kernel(int P, int mode)
         DGV_PICK(1)
         DGV_PICK(8)
         DGV_PICK(27)
+    case 125:  // slices of 25 basis functions per CTA
+        if (mode == MODE_F64) return k_collide_pipe<P_SLICE, MODE_F64, true>;
+        if (mode == MODE_F32C) return k_collide_pipe<P_SLICE, MODE_F32C, true>;
+        return k_collide_pipe<P_SLICE, MODE_BILINEAR, true>;
     default: return nullptr;
     }
 #undef DGV_PICK
 }
+
+// basis functions per CTA of the sliced kernels, and the slices of a grid
+static int p_slices(int P) { return P > 27 ? (P + P_SLICE - 1) / P_SLICE : 1; }
 
 struct LaunchShape {
     int dcta, slices, threads, nst, sp, off_f, off_hdr, off_bar;
@@ -310,7 +338,7 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     Layout &L = c->lay;
     const int mode = d_f2 ? MODE_BILINEAR : (precision == DGV_PREC_F64 ? MODE_F64 : MODE_F32C);
     KernelFn fn = pick_kernel(g.P, mode);
-    if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8 or 27 nodes per cell");
+    if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8, 27 or 125 nodes per cell");
     LaunchShape sh;
     int rc = shape_for(c, mode, sh, cell1 - cell0);
     if (rc) return rc;
@@ -333,11 +361,12 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     a.nchunks = nchunks; a.dcta = sh.dcta; a.nst = sh.nst; a.sp = sh.sp;
     a.cell0 = cell0; a.cell1 = cell1;
     a.off_f = sh.off_f; a.off_hdr = sh.off_hdr; a.off_bar = sh.off_bar;
+    a.Pt = g.P; a.npsl = p_slices(g.P);
     // VDF fastest: the CTAs resident at one time work on the same chunk of
     // rows for different VDFs, so each row is fetched from HBM once and then
     // served from L2
     KTimer kt(c);
-    fn<<<dim3(nvdf, sh.slices, nchunks), sh.threads, sh.smem, c->stream>>>(a);
+    fn<<<dim3(nvdf, sh.slices * a.npsl, nchunks), sh.threads, sh.smem, c->stream>>>(a);
     kt.stop(1);
     DGV_CUDA(c, cudaGetLastError());
     const long long tot_out = (long long)nvdf * (cell1 - cell0) * g.P;
@@ -364,7 +393,7 @@ static int choose_chunks(Ctx *c, const double *d_f, const double *d_f2, double *
     if (rc0) return 1;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    long long units = (long long)nvdf * sh.slices;
+    long long units = (long long)nvdf * sh.slices * p_slices(c->grid.P);
     if (units * 4 >= nsm) {
         for (int k = 1; k <= 64; k++) {
             long long ctas = units * k;

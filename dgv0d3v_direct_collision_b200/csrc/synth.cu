@@ -15,6 +15,7 @@
 // with a seeded stand-in for the collision integral.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -99,51 +100,66 @@ __global__ void k_synth_count(SynthArgs s, int *counts)
     }
 }
 
-// one CTA per non-empty block; P*P <= blockDim.x; pairs written in (l1,l2) order
+// one CTA per non-empty block; pairs written in (l1,l2) order, in chunks of
+// blockDim.x candidate pairs (a multiple of 32) with a running base
 __global__ void k_synth_fill(SynthArgs s, const BlockInfo *blk, double *rows64, int RD64, float *rows32,
                              int RW32)
 {
     const BlockInfo b = blk[blockIdx.x];
-    const int P = s.P, t = threadIdx.x;
-    int l1 = t / P, l2 = t - l1 * P;
-    double dsph = -1.0;
-    if (t < P * P && !(b.c1 == b.c2 && l2 <= l1)) dsph = pair_passes(s, b.c1 * P + l1, b.c2 * P + l2);
-    const bool pass = dsph >= 0.0;
-    // exclusive rank of this pair among passing pairs, in thread order
+    const int P = s.P;
     __shared__ int wsum[32];
-    unsigned m = __ballot_sync(0xffffffffu, pass);
-    int lane = t & 31, w = t >> 5;
-    int rank = __popc(m & ((1u << lane) - 1u));
-    if (lane == 0) wsum[w] = __popc(m);
+    __shared__ int chunk_base;
+    if (threadIdx.x == 0) chunk_base = 0;
     __syncthreads();
-    int base = 0;
-    for (int k = 0; k < w; k++) base += wsum[k];
-    if (!pass) return;
-    long long k = b.start + base + rank;
-    int a = b.c1 * P + l1, bb = b.c2 * P + l2;
-    int o[2] = {l1 * s.Nc + (b.c1 - s.ccell), l2 * s.Nc + (b.c2 - s.ccell)};
-    double *r = rows64 + (size_t)k * RD64;
-    float *r32 = rows32 + (size_t)k * RW32;
-    double slot;
-    memcpy(&slot, o, 8);
-    r[0] = slot;
-    r32[0] = __int_as_float(o[0]);
-    r32[1] = __int_as_float(o[1]);
-    double w2 = s.nwt[a], w3 = s.nwt[bb];
-    for (int p = 0; p < P; p++) {
-        double v = synth_value(s.seed, p, a, bb, w2, w3, dsph);
-        r[1 + p] = v;
-        r32[2 + p] = __double2float_rn(v);
+    for (int t0 = 0; t0 < P * P; t0 += blockDim.x) {
+        const int t = t0 + (int)threadIdx.x;
+        const int l1 = t / P, l2 = t - l1 * P;
+        double dsph = -1.0;
+        if (t < P * P && !(b.c1 == b.c2 && l2 <= l1)) dsph = pair_passes(s, b.c1 * P + l1, b.c2 * P + l2);
+        const bool pass = dsph >= 0.0;
+        // exclusive rank of this pair among passing pairs, in thread order
+        const unsigned m = __ballot_sync(0xffffffffu, pass);
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const int rank = __popc(m & ((1u << lane) - 1u));
+        if (lane == 0) wsum[w] = __popc(m);
+        __syncthreads();
+        int base = chunk_base;
+        for (int k = 0; k < w; k++) base += wsum[k];
+        if (pass) {
+            const long long k = b.start + base + rank;
+            const int a = b.c1 * P + l1, bb = b.c2 * P + l2;
+            int o[2] = {l1 * s.Nc + (b.c1 - s.ccell), l2 * s.Nc + (b.c2 - s.ccell)};
+            double *r = rows64 + (size_t)k * RD64;
+            float *r32 = rows32 + (size_t)k * RW32;
+            double slot;
+            memcpy(&slot, o, 8);
+            r[0] = slot;
+            r32[0] = __int_as_float(o[0]);
+            r32[1] = __int_as_float(o[1]);
+            const double w2 = s.nwt[a], w3 = s.nwt[bb];
+            for (int p = 0; p < P; p++) {
+                const double v = synth_value(s.seed, p, a, bb, w2, w3, dsph);
+                r[1 + p] = v;
+                r32[2 + p] = __double2float_rn(v);
+            }
+            for (int p = 1 + P; p < RD64; p++) r[p] = 0.0;
+            for (int p = 2 + P; p < RW32; p++) r32[p] = 0.0f;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); k++) tot += wsum[k];
+            chunk_base += tot;
+        }
+        __syncthreads();
     }
-    for (int p = 1 + P; p < RD64; p++) r[p] = 0.0;
-    for (int p = 2 + P; p < RW32; p++) r32[p] = 0.0f;
 }
 
 int layout_synthetic(Ctx *c, unsigned long long seed, double Trad, int support_mode)
 {
     const Grid &g = c->grid;
     const int P = g.P, Nc = g.Nc;
-    if (P * P > 1024) return set_err(c, DGV_EUNSUP, "synthetic A: at most 32 nodes per cell");
+    if (P > 255) return set_err(c, DGV_EUNSUP, "synthetic A: at most 255 nodes per cell");
     if (support_mode != 0 && support_mode != 1) return set_err(c, DGV_EINVAL, "synthetic A: support_mode is 0 or 1");
     if (!(Trad > 0.0)) return set_err(c, DGV_EINVAL, "synthetic A: Trad must be positive");
     SynthArgs s;
@@ -218,7 +234,7 @@ int layout_synthetic(Ctx *c, unsigned long long seed, double Trad, int support_m
     DGV_CUDA(c, cudaMalloc(&L.rows32, std::max<long long>(1, npairs) * L.RW32 * sizeof(float)));
     if (!blk.empty()) {
         DGV_CUDA(c, cudaMemcpyAsync(L.blk, blk.data(), blk.size() * sizeof(BlockInfo), cudaMemcpyHostToDevice, c->stream));
-        int fthr = ((P * P + 31) / 32) * 32;
+        const int fthr = std::min(1024, ((P * P + 31) / 32) * 32);
         k_synth_fill<<<(unsigned)blk.size(), fthr, 0, c->stream>>>(s, L.blk, (double *)L.rows64, L.RD64,
                                                                     (float *)L.rows32, L.RW32);
         DGV_CUDA(c, cudaGetLastError());
