@@ -259,13 +259,17 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def load_profile_traffic(form: int):
+def load_profile_traffic(form: int, set_mb: int = 0):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/k_collide_tc2_27cubed_b256.json for the block form,
-    k_collide_tc_27cubed_b256.json for the chunk form), or None."""
+    summary (profiles/k_collide_tc2_27cubed_b256.json for the block form, per
+    MB of block records per launch; k_collide_tc_27cubed_b256.json for the
+    chunk form), or None."""
     name = "k_collide_tc2_27cubed_b256.json" if form == 2 else "k_collide_tc_27cubed_b256.json"
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", name)))
+        if "dram_bytes_per_launch_by_set_mb" in d:
+            v = d["dram_bytes_per_launch_by_set_mb"].get(str(set_mb))
+            return (float(v) if v is not None else None), d.get("note", "")
         return float(d["dram_bytes_per_launch"]), d.get("note", "")
     except Exception:
         return None, ""
@@ -304,6 +308,10 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
     t_prep = time.perf_counter() - t
     plan = solver.tc_plan(BATCH)  # the records and lists exist now
+    from dgv0d3v_direct_collision_b200._lib import DGV_OPT_TCSETMB, DGV_OPT_TCTILES
+    tc_launch = {"tiles_per_cta": solver.get_option(DGV_OPT_TCTILES),
+                 "set_mb": solver.get_option(DGV_OPT_TCSETMB),
+                 "chosen_by": "the library's autotuner" if not (args.tc_tiles or args.tc_set_mb) else "options"}
     solver.set_kernel_timing(True)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup - 1):
@@ -413,7 +421,7 @@ def run_ours(args, world, rank, local):
     # FLOPs the MMAs issue per launch (dense tiles, three split products) over the same time
     issued = plan["tensor_flop"] / max(plan["launches"], 1) / (k_ms_launch / 1000.0) / 1e12
     form = solver.tc_form
-    traffic, tnote = load_profile_traffic(form)
+    traffic, tnote = load_profile_traffic(form, tc_launch["set_mb"])
     kname = "k_collide_tc2<128,27>" if form == 2 else "k_collide_tc<128>"
     knote = ("algorithmic FLOPs = 3 per record-shift (A*f*f + add) x VDFs; the block form computes "
              "G = f(c2) W per cell-pair block on the tensor core (dense W: 27 x 729 per block, 3 fp16 "
@@ -435,7 +443,8 @@ def run_ours(args, world, rank, local):
                    "record_shifts_per_eval": info["record_shifts"],
                    "l2": "inputs larger than L2: the A records (~14.6 GB block form / ~8 GB chunk form) "
                          "are streamed from HBM every step",
-                   "parallelism": f"replicas over VDFs, dp{world}"},
+                   "parallelism": f"replicas over VDFs, dp{world}",
+                   "tc_launch": tc_launch},
         "f64_plain_evals_per_s": value64, "f64_timed_vdfs": NB64, "tc_over_f64": value / value64,
         "err_tc_vs_f64_norm_max": float(errs.max()), "err_tc_vs_f64_maxabs_rel_max": float(merrs.max()),
         "conservation_rel_max": float(cons),
@@ -572,7 +581,7 @@ def run_trajectory(args):
         "wall_s": wall}))
 
 
-def run_profile_case(case: str):
+def run_profile_case(case: str, args=None):
     """Cases for profiler captures.  "<prec>_21": the 21^3 grid (s=3, M=7,
     [-6,6]^3; A rows ~5.6 GB in total) -- one VDF with a fixed chunk count (no
     tuning launches) for the CUDA-core kernels, a batch of 256 VDFs for the
@@ -592,6 +601,10 @@ def run_profile_case(case: str):
     if prec == "tc2":
         s.set_tc_form(2)
         prec = "tc"
+    if args is not None and args.tc_set_mb:
+        s.set_tc_set_mb(args.tc_set_mb)
+    if args is not None and args.tc_tiles:
+        s.set_tc_tiles_per_cta(args.tc_tiles)
     if prec not in ("tc", "vjptc"):
         s.set_nchunks(296)
     nb = BATCH if prec in ("tc", "vjptc") else 1
@@ -643,7 +656,7 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.profile_case:
-        run_profile_case(args.profile_case)
+        run_profile_case(args.profile_case, args)
         return
     if args.mixed:
         run_mixed(args)

@@ -22,7 +22,7 @@ STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4
 # every entry point include/dgv_b200.h declares
 EXPORTS = [
     "dgv_ctx_create", "dgv_ctx_destroy", "dgv_last_error", "dgv_set_stream", "dgv_set_async",
-    "dgv_set_option", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
+    "dgv_set_option", "dgv_get_option", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper", "dgv_set_regime",
     "dgv_regime_info",
     "dgv_step_rk", "dgv_step_rk_batched", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
@@ -101,6 +101,7 @@ def load() -> C.CDLL:
         "dgv_jvp": [vp, vp, vp, vp, C.c_int],
         "dgv_vjp": [vp, vp, vp, vp, C.c_int],
         "dgv_vjp_batched": [vp, i32, vp, vp, vp, C.c_int],
+        "dgv_get_option": [vp, C.c_int, C.POINTER(C.c_int64)],
         "dgv_prepare_linear": [vp, vp],
         "dgv_apply_linear": [vp, vp, vp, C.c_int],
         "dgv_collide_f64_noalloc": [vp, vp, vp, i32, vp],

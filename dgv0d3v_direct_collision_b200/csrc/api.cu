@@ -371,6 +371,25 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
     }
 }
 
+int dgv_get_option(dgv_ctx *ctx, int option, int64_t *value)
+{
+    CTX_CHECK(ctx);
+    const Ctx &c = ctx->c;
+    if (!value) return set_err(&ctx->c, DGV_EINVAL, "get_option: NULL value");
+    switch (option) {
+    case DGV_OPT_PROJECT: *value = c.project ? 1 : 0; return DGV_OK;
+    case DGV_OPT_NCHUNKS: *value = c.nchunks_opt; return DGV_OK;
+    case DGV_OPT_KTIMING: *value = c.ktiming ? 1 : 0; return DGV_OK;
+    case DGV_OPT_TCFORM: *value = c.tc_form; return DGV_OK;
+    case DGV_OPT_TCTILES: *value = c.tc_tiles_per_cta; return DGV_OK;
+    case DGV_OPT_TCSETMB: *value = c.tc_set_mb; return DGV_OK;
+    case DGV_OPT_WAIT_LIMIT_US: *value = c.wait_limit_us; return DGV_OK;
+    case DGV_OPT_TCAUTOTUNE: *value = c.tc_autotune ? 1 : 0; return DGV_OK;
+    case DGV_OPT_TEST_WITHHOLD: *value = c.test_withhold ? 1 : 0; return DGV_OK;
+    default: return set_err(&ctx->c, DGV_EINVAL, "unknown option");
+    }
+}
+
 int dgv_kernel_stats(dgv_ctx *ctx, double *ms, int64_t *launches, int64_t *all_launches, int reset)
 {
     CTX_CHECK(ctx);

@@ -1337,6 +1337,28 @@ static void tc2_sets(Ctx *c)
     }
     if (L.tc2_sets.back() != (int)L.nblocks) L.tc2_sets.push_back((int)L.nblocks);
     L.tc2_set_mb = c->tc_set_mb;
+    L.tc2_sets_adj.clear();
+}
+
+// The adjoint's launches: about tc_set_mb MB of records per launch counting
+// both record sets its items read (W for the pass to the c1 side, W2 for
+// the pass to the c2 side), so that a launch's records stay in L2 as the
+// collision operator's do.  Built after tc2_sets and the adjoint's records.
+static void tc2_sets_adjoint(Ctx *c)
+{
+    Layout &L = c->lay;
+    if (!L.tc2_sets_adj.empty()) return;
+    L.tc2_sets_adj.push_back(0);
+    const long long per_set = std::max<long long>(1, ((long long)c->tc_set_mb << 20) / T2_GREC);
+    long long acc = 0;
+    for (long long b = 0; b < L.nblocks; b++) {
+        acc += (L.tc2_goff[b + 1] - L.tc2_goff[b]) + (L.tc2_goff2[b + 1] - L.tc2_goff2[b]);
+        if (acc >= per_set && b + 1 < L.nblocks) {
+            L.tc2_sets_adj.push_back((int)(b + 1));
+            acc = 0;
+        }
+    }
+    if (L.tc2_sets_adj.back() != (int)L.nblocks) L.tc2_sets_adj.push_back((int)L.nblocks);
 }
 
 // the wait limit of the launches, and the one-shot test switch (DGV_OPT_TEST_WITHHOLD:
@@ -1350,32 +1372,32 @@ static void tc2_wait_args(Ctx *c, Tc2Args &a)
 }
 
 template <int VB, int P, int MODE = 0>
-static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng)
+static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, const std::vector<int> &sets)
 {
     const size_t smem = (size_t)T2_NSTW * T2_GREC + 4 * (size_t)a.region + (2 * T2_NSTW + 13) * sizeof(uint64_t) + 16;
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc2<VB, P, MODE>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const Layout &L = c->lay;
     KTimer kt(c);
-    for (size_t s = 0; s + 1 < L.tc2_sets.size(); s++) {
+    for (size_t s = 0; s + 1 < sets.size(); s++) {
         a.item_start = tl.item_start + s * (ng + 1);
         a.tile_of = tl.tile_of + s * ng;
         k_collide_tc2<VB, P, MODE><<<(unsigned)(a.nbp * ng), T2_THREADS, smem, c->stream>>>(a);
         DGV_CUDA(c, cudaGetLastError());
         a.withhold = 0;  // the test withholds in the first launch only
     }
-    kt.stop((long long)L.tc2_sets.size() - 1);
-    count_launches(c, (long long)L.tc2_sets.size() - 1);
+    kt.stop((long long)sets.size() - 1);
+    count_launches(c, (long long)sets.size() - 1);
     return DGV_OK;
 }
 
 template <int P, int MODE = 0>
-static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, int VB)
+static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, int VB, const std::vector<int> &sets)
 {
     switch (VB) {
-    case 128: return launch_tc2<128, P, MODE>(c, a, tl, ng);
-    case 64: return launch_tc2<64, P, MODE>(c, a, tl, ng);
-    default: return launch_tc2<32, P, MODE>(c, a, tl, ng);
+    case 128: return launch_tc2<128, P, MODE>(c, a, tl, ng, sets);
+    case 64: return launch_tc2<64, P, MODE>(c, a, tl, ng, sets);
+    default: return launch_tc2<32, P, MODE>(c, a, tl, ng, sets);
     }
 }
 
@@ -1419,7 +1441,7 @@ static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, do
     a.nbp = (nbt + a.tpc - 1) / a.tpc;
     a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
     tc2_wait_args(c, a);
-    rc = g.P == 27 ? launch_tc2_vb<27>(c, a, tl, ng, VB) : launch_tc2_vb<8>(c, a, tl, ng, VB);
+    rc = g.P == 27 ? launch_tc2_vb<27>(c, a, tl, ng, VB, L.tc2_sets) : launch_tc2_vb<8>(c, a, tl, ng, VB, L.tc2_sets);
     if (rc) return rc;
     long long tot = (long long)nvdf * g.N;
     k_tc_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, c->d_nwt, d_q, g.N, nvdf, NV, scale);
@@ -1604,6 +1626,7 @@ int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int
     if (rc) return rc;
     if ((rc = tc2_prepare_adjoint(c))) return rc;
     tc2_sets(c);
+    tc2_sets_adjoint(c);
     if ((rc = ensure_errflag(c))) return rc;
     const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), NDG = TC_ROWS / VB;
     const int nbt = (nvdf + VB - 1) / VB, NV = nbt * VB, ng = (g.Nc + NDG - 1) / NDG;
@@ -1617,7 +1640,7 @@ int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int
     TcLists tl;
     {
         std::vector<int> first, count;
-        rc = tc_work_lists(c, NDG, 512 + NDG, L.tc2_sets, first, count, &tl, 2);
+        rc = tc_work_lists(c, NDG, 512 + NDG, L.tc2_sets_adj, first, count, &tl, 2);
         if (rc) return rc;
     }
     float *F = reinterpret_cast<float *>(c->d_tcF);
@@ -1640,7 +1663,8 @@ int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int
     a.nbp = (nbt + a.tpc - 1) / a.tpc;
     a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
     tc2_wait_args(c, a);
-    rc = g.P == 27 ? launch_tc2_vb<27, 1>(c, a, tl, ng, VB) : launch_tc2_vb<8, 1>(c, a, tl, ng, VB);
+    rc = g.P == 27 ? launch_tc2_vb<27, 1>(c, a, tl, ng, VB, L.tc2_sets_adj)
+                   : launch_tc2_vb<8, 1>(c, a, tl, ng, VB, L.tc2_sets_adj);
     if (rc) return rc;
     const long long tot = (long long)nvdf * g.N;
     k_tc_vjp_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, inv_f, inv_c, d_g, g.N, nvdf, NV);

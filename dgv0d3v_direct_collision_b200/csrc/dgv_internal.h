@@ -77,6 +77,7 @@ struct Layout {
     void *tc2_Wv = nullptr;  // device: the adjoint's second record set (built on first use)
     double tc2_vscale = 1.0;
     std::vector<int> tc2_sets;
+    std::vector<int> tc2_sets_adj;  // the adjoint's launches (both of its record sets per launch)
     int tc2_set_mb = 0;  // record megabytes per set the sets were built for
     // device work lists {items, item starts, tile order}, keyed by cells per
     // tile (chunk form) or 256 + cells per tile (block form)

@@ -155,6 +155,12 @@ class DGVSolver:
         self._check(self._lib.dgv_tc_plan(self._h, int(nvdf), C.byref(l), C.byref(it), C.byref(fl)))
         return {"launches": l.value, "items": it.value, "tensor_flop": fl.value}
 
+    def get_option(self, option: int) -> int:
+        """The current value of a DGV_OPT_* option (dgv_get_option)."""
+        v = C.c_int64(0)
+        self._check(self._lib.dgv_get_option(self._h, int(option), C.byref(v)))
+        return int(v.value)
+
     def set_tc_set_mb(self, mb: int):
         """Block form: megabytes of block records per kernel launch."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCSETMB, int(mb)))

@@ -104,6 +104,10 @@ int dgv_set_stream(dgv_ctx *ctx, void *stream);
 /* 1: device-pointer calls return without synchronising the stream */
 int dgv_set_async(dgv_ctx *ctx, int async_flag);
 int dgv_set_option(dgv_ctx *ctx, int option, int64_t value);
+/* No counterpart in the reference (configuration query): the current value
+ * of an option (for DGV_OPT_TCTILES / DGV_OPT_TCSETMB: the choice the
+ * autotuner made for the last batch class evaluated) */
+int dgv_get_option(dgv_ctx *ctx, int option, int64_t *value);
 /* No counterpart in the reference (measurement hook): summed device time in
  * ms and launch count of the collision kernel (k_collide_tc / k_collide_pipe)
  * over the calls made since the last reset while DGV_OPT_KTIMING was on,
