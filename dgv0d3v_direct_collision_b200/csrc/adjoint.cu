@@ -13,10 +13,13 @@
 // local-major copy g_lm[l*Nc + cell] -- the layout of the shared copy of f,
 // so its indices are the gather offsets o1+D, o2+D -- where the 32 lanes of
 // a warp (32 consecutive cells) hit 256 contiguous bytes instead of 32 lines
-// P doubles apart; k_lm_to_nodes writes g in node order afterwards.
+// P doubles apart; k_lm_to_nodes writes g in node order afterwards.  On grids
+// whose f does not fit in shared memory (or with DGV_OPT_FGLOBAL) the gathers
+// read a local-major copy of f in global memory instead (GF).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "dgv_internal.h"
 #include "pipeline.cuh"
@@ -33,13 +36,15 @@ struct VjpArgs {
     long long N;
     int Nc, Mv, Mw, dcta, rowb, nst, sp, off_f, off_hdr, off_bar;
     int Pt, npsl;  // nodes per cell; slices of PV basis functions (1 unless sliced)
+    const double *fg;  // GF: local-major copy of f
+    unsigned long long wait_ns;  // limit of every bounded wait
 };
 
 // Same shared-memory row pipeline as the forward kernel (pipeline.cuh).
 // SL (sliced, for many nodes per cell): a CTA forms vA over the PV basis
 // functions of its slice only (blockIdx.y % npsl) and scatters that part;
 // the scatters of the slices add up to the full adjoint.
-template <int PV, bool SL = false>
+template <int PV, bool SL = false, bool GF = false>
 __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -59,17 +64,22 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
         }
         fence_mbar_init();
     }
-    for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
-        int cell = (int)(i / PT), l = (int)(i - (long long)cell * PT);
-        f_s[l * a.Nc + cell] = __ldg(a.f + i);
+    auto fat = [&](int q) -> double {
+        if constexpr (GF) return __ldg(a.fg + q);
+        else return f_s[q];
+    };
+    if constexpr (!GF) {
+        for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
+            int cell = (int)(i / PT), l = (int)(i - (long long)cell * PT);
+            f_s[l * a.Nc + cell] = __ldg(a.f + i);
+        }
     }
     __syncthreads();
     const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
     const int d0 = slice * a.dcta, d1 = min(a.Nc, d0 + a.dcta);
-    if (threadIdx.x < 32) {  // producer: lane 0 of warp 0
-        if (threadIdx.x == 0)
-            produce_rows(a.blk, b0, b1, a.Mv, a.Mw, d0, d1, a.rows, a.rowb, stages, a.sp, a.nst, hdr, full, empty,
-                         a.err);
+    if (threadIdx.x < 32) {  // producer: warp 0
+        produce_rows(a.blk, b0, b1, a.Mv, a.Mw, d0, d1, a.rows, a.rowb, stages, a.sp, a.nst, hdr, full, empty, a.err,
+                     a.wait_ns);
         return;
     }
     const int tc = threadIdx.x - 32, lane = threadIdx.x & 31;
@@ -87,7 +97,7 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
     bool valid = false;
     for (int it = 0;; it++) {
         const int s = it % a.nst;
-        if (!mbar_wait(&full[s], (it / a.nst) & 1, a.err)) break;
+        if (!mbar_wait(&full[s], (it / a.nst) & 1, a.err, a.wait_ns)) break;
         const StageHdr h = hdr[s];
         if (h.block < 0) break;
         if (h.block != cur) {
@@ -121,8 +131,8 @@ __global__ void __launch_bounds__(384, 1) k_vjp_pipe(VjpArgs a)
                     for (int j = 0; j < PV; j++) vA = fma(rv[1 + j], cw[j], vA);
                 }
                 const int q1 = (int)(unsigned)(o & 0xffffffffLL) + D, q2 = (int)(o >> 32) + D;
-                atomicAdd(a.g + q1, vA * f_s[q2]);
-                atomicAdd(a.g + q2, vA * f_s[q1]);
+                atomicAdd(a.g + q1, vA * fat(q2));
+                atomicAdd(a.g + q2, vA * fat(q1));
             }
         }
         __syncwarp();
@@ -147,14 +157,7 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     if (!c->lay.blk) return set_err(c, DGV_ESTATE, "vjp: no A-arrays loaded");
     const Grid &g = c->grid;
     const Layout &L = c->lay;
-    VjpFn fn = nullptr;
-    switch (g.P) {
-    case 1: fn = k_vjp_pipe<1>; break;
-    case 8: fn = k_vjp_pipe<8>; break;
-    case 27: fn = k_vjp_pipe<27>; break;
-    case 125: fn = k_vjp_pipe<25, true>; break;  // slices of 25 basis functions per CTA
-    default: return set_err(c, DGV_EUNSUP, "vjp: this build supports 1, 8, 27 or 125 nodes per cell");
-    }
+    if (g.N > INT32_MAX / 2) return set_err(c, DGV_EUNSUP, "vjp: grid too large");
     const int npsl = g.P > 27 ? (g.P + 24) / 25 : 1;
     int maxsm = 0, nsm = 148;
     DGV_CUDA(c, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
@@ -162,10 +165,22 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     const int slices = (g.Nc + 351) / 352;
     const int dcta = ((g.Nc + slices - 1) / slices + 31) / 32 * 32;
     const int rowb = L.RD64 * 8, nst = 6;
-    const size_t fbytes = (size_t)g.N * sizeof(double);
+    size_t fbytes = (size_t)g.N * sizeof(double);
     const size_t tail = 16 + nst * sizeof(StageHdr) + 2 * nst * sizeof(uint64_t) + 16;
+    const bool gf = c->f_global == 1 || fbytes + tail + (size_t)nst * 4 * rowb > (size_t)maxsm;
+    if (gf) fbytes = 0;
     if (fbytes + tail + (size_t)nst * 4 * rowb > (size_t)maxsm)
-        return set_err(c, DGV_EUNSUP, "vjp: f does not fit in shared memory for this grid");
+        return set_err(c, DGV_EUNSUP, "vjp: the row ring does not fit in shared memory");
+    VjpFn fn = nullptr;
+#define DGV_VJP_PICK(...) fn = gf ? k_vjp_pipe<__VA_ARGS__, true> : k_vjp_pipe<__VA_ARGS__, false>
+    switch (g.P) {
+    case 1: DGV_VJP_PICK(1, false); break;
+    case 8: DGV_VJP_PICK(8, false); break;
+    case 27: DGV_VJP_PICK(27, false); break;
+    case 125: DGV_VJP_PICK(25, true); break;  // slices of 25 basis functions per CTA
+    default: return set_err(c, DGV_EUNSUP, "vjp: this build supports 1, 8, 27 or 125 nodes per cell");
+    }
+#undef DGV_VJP_PICK
     const size_t ring = std::min<size_t>(64 * 1024, (size_t)maxsm - fbytes - tail);
     const int sp = (int)std::min<size_t>(256, ring / ((size_t)nst * rowb));
     VjpArgs a;
@@ -186,6 +201,13 @@ int vjp_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int pr
     a.f = d_f; a.v = d_v; a.w = c->d_nwt; a.g = c->d_glm; a.blk = L.blk; a.rows = (const char *)L.rows64;
     a.bounds = d_bounds; a.err = c->d_err; a.N = g.N; a.Nc = g.Nc; a.Mv = g.d.Mv; a.Mw = g.d.Mw; a.dcta = dcta;
     a.rowb = rowb; a.nst = nst; a.sp = sp; a.Pt = g.P; a.npsl = npsl;
+    a.wait_ns = wait_limit_ns(c);
+    a.fg = nullptr;
+    if (gf) {
+        const void *fg = nullptr;
+        if ((rc = f_local_major(c, d_f, 1, false, &fg))) return rc;
+        a.fg = static_cast<const double *>(fg);
+    }
     fn<<<dim3(1, slices * npsl, nchunks), 32 + dcta, smem, c->stream>>>(a);
     DGV_CUDA(c, cudaGetLastError());
     k_lm_to_nodes<<<(unsigned)((g.N + 255) / 256), 256, 0, c->stream>>>(c->d_glm, d_g, g.N, g.Nc, g.P);

@@ -7,7 +7,10 @@
 // output cells x one VDF):
 //   * f of the VDF is staged once into shared memory, local-major
 //     f_s[l*Nc + cell], so that the 32 lanes of a warp (32 consecutive output
-//     cells D) gather 32 consecutive words: conflict-free;
+//     cells D) gather 32 consecutive words: conflict-free; on grids whose f
+//     does not fit (FP64: more than ~26 000 nodes), the gathers read a
+//     local-major copy in global memory instead (GF: 256 contiguous bytes per
+//     warp and gather, served by L1 and L2);
 //   * every thread owns one output cell D and keeps the P sums of its P
 //     output nodes (D, p) in registers;
 //   * a block's pairs are streamed with warp-uniform broadcast loads of their
@@ -48,6 +51,8 @@ struct CollideArgs {
     int nst, sp;            // pipeline stages, pairs per stage
     int off_f, off_hdr, off_bar;  // shared-memory layout (bytes)
     int Pt, npsl;           // nodes per cell; slices of PV basis functions per cell (1 unless sliced)
+    const void *fg;         // GF: local-major copies of f, [nvdf][Pt*Nc] of the kernel's type
+    unsigned long long wait_ns;  // limit of every bounded wait
 };
 
 // Knuth's branch-free two-sum: s + c carries x exactly
@@ -73,7 +78,9 @@ __device__ __forceinline__ void two_sum_acc(float &s, float &c, float x)
 // basis functions p in [ps*PV, ps*PV + PV) of its output cells (ps =
 // blockIdx.y % npsl), reading them from the full rows with scalar loads; the
 // node stride is the runtime Pt.
-template <int PV, int MODE, bool SL = false>
+// GF (f in global memory): the gathers read a.fg, a local-major copy of f made
+// by k_f_local_major, instead of a shared-memory copy.
+template <int PV, int MODE, bool SL = false, bool GF = false>
 __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
 {
     using T = typename std::conditional<MODE == MODE_F32C, float, double>::type;
@@ -95,19 +102,26 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
         }
         fence_mbar_init();
     }
-    const double *f = a.f + (size_t)vdf * a.N;
-    for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
-        int cell = (int)(i / PT), l = (int)(i - (long long)cell * PT);
-        f_s[l * a.Nc + cell] = (T)__ldg(f + i);
+    const T *fgv = GF ? reinterpret_cast<const T *>(a.fg) + (size_t)vdf * a.N : nullptr;
+    // f at local-major index q (l*Nc + cell)
+    auto fat = [&](int q) -> T {
+        if constexpr (GF) return __ldg(fgv + q);
+        else return f_s[q];
+    };
+    if constexpr (!GF) {
+        const double *f = a.f + (size_t)vdf * a.N;
+        for (long long i = threadIdx.x; i < a.N; i += blockDim.x) {
+            int cell = (int)(i / PT), l = (int)(i - (long long)cell * PT);
+            f_s[l * a.Nc + cell] = (T)__ldg(f + i);
+        }
     }
     __syncthreads();
     const int b0 = a.bounds[chunk], b1 = a.bounds[chunk + 1];
     const int d0 = a.cell0 + slice * a.dcta, d1 = min(a.cell1, d0 + a.dcta);
 
-    if (threadIdx.x < 32) {  // producer: lane 0 of warp 0
-        if (threadIdx.x == 0)
-            produce_rows(a.blk, b0, b1, a.Mv, a.Mw, d0, d1, a.rows, a.rowb, stages, a.sp, a.nst, hdr, full, empty,
-                         a.err);
+    if (threadIdx.x < 32) {  // producer: warp 0
+        produce_rows(a.blk, b0, b1, a.Mv, a.Mw, d0, d1, a.rows, a.rowb, stages, a.sp, a.nst, hdr, full, empty, a.err,
+                     a.wait_ns);
         return;
     }
 
@@ -132,7 +146,7 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
     constexpr int RW = ((2 + PV) + 3) / 4 * 4;  // FP32 row, words
     for (int it = 0;; it++) {
         const int s = it % a.nst;
-        if (!mbar_wait(&full[s], (it / a.nst) & 1, a.err)) break;
+        if (!mbar_wait(&full[s], (it / a.nst) & 1, a.err, a.wait_ns)) break;
         const StageHdr h = hdr[s];
         if (h.block < 0) break;
         if (h.block != cur) {
@@ -156,12 +170,12 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
             if constexpr (MODE == MODE_F32C) {
                 const int *ow = reinterpret_cast<const int *>(st);
                 const int rws = a.rowb / 4;
-                float pa = f_s[ow[0] + D], pb = f_s[ow[1] + D];
+                float pa = fat(ow[0] + D), pb = fat(ow[1] + D);
                 for (int k = 0; k < h.n; k++) {
                     const float prod = pa * pb;
                     if (k + 1 < h.n) {
-                        pa = f_s[ow[(k + 1) * rws] + D];
-                        pb = f_s[ow[(k + 1) * rws + 1] + D];
+                        pa = fat(ow[(k + 1) * rws] + D);
+                        pb = fat(ow[(k + 1) * rws + 1] + D);
                     }
                     if constexpr (SL) {
                         const float *rowf = reinterpret_cast<const float *>(st + (size_t)k * a.rowb) + 2 + pofs;
@@ -188,7 +202,7 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
                 const int *ow = reinterpret_cast<const int *>(st);
                 const int rws = a.rowb / 4;
                 int q1 = ow[0] + D, q2 = ow[1] + D;
-                double pa = f_s[q1], pb = f_s[q2];
+                double pa = fat(q1), pb = fat(q2);
                 double ga = 0.0, gb = 0.0;
                 if constexpr (MODE == MODE_BILINEAR) {
                     const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
@@ -202,8 +216,8 @@ __global__ void __launch_bounds__(384, 1) k_collide_pipe(CollideArgs a)
                     if (k + 1 < h.n) {
                         q1 = ow[(k + 1) * rws] + D;
                         q2 = ow[(k + 1) * rws + 1] + D;
-                        pa = f_s[q1];
-                        pb = f_s[q2];
+                        pa = fat(q1);
+                        pb = fat(q2);
                         if constexpr (MODE == MODE_BILINEAR) {
                             const int l1 = q1 / a.Nc, l2 = q2 / a.Nc;
                             ga = __ldg(g + (long long)(q1 - l1 * a.Nc) * PT + l1);
@@ -273,37 +287,77 @@ __global__ void k_reduce_chunks(const double *partial, const double *w, double *
 // -------------------------------------------------------------------------
 typedef void (*KernelFn)(CollideArgs);
 
-static KernelFn pick_kernel(int P, int mode)
+template <bool GF>
+static KernelFn pick_kernel_gf(int P, int mode)
 {
-#define DGV_PICK(PV)                                              \
-    case PV:                                                      \
-        if (mode == MODE_F64) return k_collide_pipe<PV, MODE_F64>;  \
-        if (mode == MODE_F32C) return k_collide_pipe<PV, MODE_F32C>; \
-        return k_collide_pipe<PV, MODE_BILINEAR>;
+#define DGV_PICK(PV)                                                           \
+    case PV:                                                                   \
+        if (mode == MODE_F64) return k_collide_pipe<PV, MODE_F64, false, GF>;   \
+        if (mode == MODE_F32C) return k_collide_pipe<PV, MODE_F32C, false, GF>; \
+        return k_collide_pipe<PV, MODE_BILINEAR, false, GF>;
     switch (P) {
         DGV_PICK(1)
         DGV_PICK(8)
         DGV_PICK(27)
     case 125:  // slices of 25 basis functions per CTA
-        if (mode == MODE_F64) return k_collide_pipe<P_SLICE, MODE_F64, true>;
-        if (mode == MODE_F32C) return k_collide_pipe<P_SLICE, MODE_F32C, true>;
-        return k_collide_pipe<P_SLICE, MODE_BILINEAR, true>;
+        if (mode == MODE_F64) return k_collide_pipe<P_SLICE, MODE_F64, true, GF>;
+        if (mode == MODE_F32C) return k_collide_pipe<P_SLICE, MODE_F32C, true, GF>;
+        return k_collide_pipe<P_SLICE, MODE_BILINEAR, true, GF>;
     default: return nullptr;
     }
 #undef DGV_PICK
 }
 
+static KernelFn pick_kernel(int P, int mode, bool gf)
+{
+    return gf ? pick_kernel_gf<true>(P, mode) : pick_kernel_gf<false>(P, mode);
+}
+
+// out[v][l*Nc + cell] = (T) f[v][cell*P + l]: the local-major copies the GF
+// kernels gather from (reads coalesced; writes strided by Nc)
+template <typename T>
+__global__ void k_f_local_major(const double *f, T *out, long long N, int Nc, int P, int nvdf)
+{
+    const long long tot = (long long)nvdf * N;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+        const long long v = i / N, r = i - v * N;
+        const int cell = (int)(r / P), l = (int)(r - (long long)cell * P);
+        out[v * N + (long long)l * Nc + cell] = (T)f[i];
+    }
+}
+
 // basis functions per CTA of the sliced kernels, and the slices of a grid
 static int p_slices(int P) { return P > 27 ? (P + P_SLICE - 1) / P_SLICE : 1; }
+
+int f_local_major(Ctx *c, const double *d_f, int nvdf, bool f32, const void **out)
+{
+    const Grid &g = c->grid;
+    int rc = ensure_buffer(c, &c->d_fg, &c->fg_bytes, (size_t)nvdf * g.N * (f32 ? sizeof(float) : sizeof(double)));
+    if (rc) return rc;
+    const long long tot = (long long)nvdf * g.N;
+    const unsigned nblk = (unsigned)std::min<long long>((tot + 255) / 256, 148LL * 16);
+    if (f32)
+        k_f_local_major<float><<<nblk, 256, 0, c->stream>>>(d_f, reinterpret_cast<float *>(c->d_fg), g.N, g.Nc, g.P,
+                                                            nvdf);
+    else
+        k_f_local_major<double><<<nblk, 256, 0, c->stream>>>(d_f, c->d_fg, g.N, g.Nc, g.P, nvdf);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 1);
+    *out = c->d_fg;
+    return DGV_OK;
+}
 
 struct LaunchShape {
     int dcta, slices, threads, nst, sp, off_f, off_hdr, off_bar;
     size_t smem;
+    bool gf;  // f gathered from a local-major copy in global memory
 };
 
 // Pipeline geometry: consumers = one warp per 32 output cells (<= 384), plus
 // the producer warp; the stage ring takes what shared memory the copy of f
-// leaves, up to 64 KiB, in 4-6 stages.
+// leaves, up to 64 KiB, in 6 stages.  f goes to global memory (GF) when its
+// shared copy and a ring of at least 4 rows per stage do not fit, or when
+// DGV_OPT_FGLOBAL asks for it.
 static int shape_for(Ctx *c, int mode, LaunchShape &s, int ncell)
 {
     const Grid &g = c->grid;
@@ -316,11 +370,15 @@ static int shape_for(Ctx *c, int mode, LaunchShape &s, int ncell)
     s.dcta = ((ncell + s.slices - 1) / s.slices + 31) / 32 * 32;
     s.threads = 32 + s.dcta;
     const int rowb = mode == MODE_F32C ? L.RW32 * 4 : L.RD64 * 8;
-    const size_t fbytes = (size_t)g.N * (mode == MODE_F32C ? sizeof(float) : sizeof(double));
+    size_t fbytes = (size_t)g.N * (mode == MODE_F32C ? sizeof(float) : sizeof(double));
     const int nst = 6;
     const size_t tail = 16 + (size_t)nst * sizeof(StageHdr) + 2 * nst * sizeof(uint64_t) + 16;
+    s.gf = c->f_global == 1 || fbytes + tail + (size_t)nst * 4 * rowb > (size_t)maxsm;
+    if (s.gf) fbytes = 0;
     if (fbytes + tail + (size_t)nst * 4 * rowb > (size_t)maxsm)
-        return set_err(c, DGV_EUNSUP, "collide: f of one VDF does not fit in shared memory for this grid");
+        return set_err(c, DGV_EUNSUP, "collide: the row ring does not fit in shared memory");
+    if (g.N > INT32_MAX / 2)  // local-major indices of the gathers are ints
+        return set_err(c, DGV_EUNSUP, "collide: grid too large");
     size_t ring = std::min<size_t>(64 * 1024, (size_t)maxsm - fbytes - tail);
     s.nst = nst;
     s.sp = (int)std::min<size_t>(256, ring / ((size_t)nst * rowb));
@@ -337,11 +395,11 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     const Grid &g = c->grid;
     Layout &L = c->lay;
     const int mode = d_f2 ? MODE_BILINEAR : (precision == DGV_PREC_F64 ? MODE_F64 : MODE_F32C);
-    KernelFn fn = pick_kernel(g.P, mode);
-    if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8, 27 or 125 nodes per cell");
     LaunchShape sh;
     int rc = shape_for(c, mode, sh, cell1 - cell0);
     if (rc) return rc;
+    KernelFn fn = pick_kernel(g.P, mode, sh.gf);
+    if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8, 27 or 125 nodes per cell");
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     nchunks = std::max(1, std::min<int>(nchunks, (int)std::max<long long>(1, L.nblocks)));
     if (nchunks > 65535) return set_err(c, DGV_EINVAL, "collide: at most 65535 chunks");
@@ -362,6 +420,9 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     a.cell0 = cell0; a.cell1 = cell1;
     a.off_f = sh.off_f; a.off_hdr = sh.off_hdr; a.off_bar = sh.off_bar;
     a.Pt = g.P; a.npsl = p_slices(g.P);
+    a.wait_ns = wait_limit_ns(c);
+    a.fg = nullptr;
+    if (sh.gf && (rc = f_local_major(c, d_f, nvdf, mode == MODE_F32C, &a.fg))) return rc;
     // VDF fastest: the CTAs resident at one time work on the same chunk of
     // rows for different VDFs, so each row is fetched from HBM once and then
     // served from L2

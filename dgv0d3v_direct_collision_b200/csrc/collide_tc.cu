@@ -1366,7 +1366,7 @@ static void tc2_sets_adjoint(Ctx *c)
 // that stage run out and the call reports DGV_ETIMEOUT)
 static void tc2_wait_args(Ctx *c, Tc2Args &a)
 {
-    a.wait_ns = c->wait_limit_us > 0 ? (unsigned long long)c->wait_limit_us * 1000ULL : WAIT_LIMIT_NS;
+    a.wait_ns = wait_limit_ns(c);
     a.withhold = c->test_withhold ? 1 : 0;
     c->test_withhold = false;
 }
@@ -1377,7 +1377,6 @@ static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, const std::
     const size_t smem = (size_t)T2_NSTW * T2_GREC + 4 * (size_t)a.region + (2 * T2_NSTW + 13) * sizeof(uint64_t) + 16;
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc2<VB, P, MODE>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const Layout &L = c->lay;
     KTimer kt(c);
     for (size_t s = 0; s + 1 < sets.size(); s++) {
         a.item_start = tl.item_start + s * (ng + 1);
@@ -1476,7 +1475,11 @@ static int tc2_autotune(Ctx *c, const double *d_f, double *d_q, int nvdf, double
     const bool kt = c->ktiming;
     const long long kt_all = c->kt_all;
     c->ktiming = false;
-    const int tiles[2] = {2, 1}, mbs[3] = {24, 48, 96};
+    // records per launch up to 48 MB: with the f tiles and the FP64
+    // accumulators a launch touches (~84 MB at 27^3 x 256), its working set
+    // then (nearly) stays in the 126 MB L2; 96 MB sets ran as fast but read
+    // their records ~10x from DRAM (measured)
+    const int tiles[2] = {2, 1}, mbs[2] = {24, 48};
     float best_ms = 1e30f;
     int best_t = c->tc_tiles_per_cta, best_mb = c->tc_set_mb, rc = DGV_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;

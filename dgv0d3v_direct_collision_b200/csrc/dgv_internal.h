@@ -118,6 +118,9 @@ struct Ctx {
     // tensor-core path: scaled fp32 copy of f (+ per-VDF scales), FP64 sums
     double *d_tcF = nullptr, *d_tcQ = nullptr;
     size_t tcF_bytes = 0, tcQ_bytes = 0;
+    // CUDA-core kernels with f in global memory: local-major copies f[v][l*Nc + cell]
+    double *d_fg = nullptr;
+    size_t fg_bytes = 0;
     // VJP: local-major accumulator g_lm[l*Nc + cell]
     double *d_glm = nullptr;
     size_t glm_bytes = 0;
@@ -144,6 +147,7 @@ struct Ctx {
     int tc_tiles_per_cta = 2;  // DGV_OPT_TCTILES: VDF tiles per CTA in the block form
     int tc_set_mb = 48;        // DGV_OPT_TCSETMB: block form, MB of records per launch
     long long wait_limit_us = 0;  // DGV_OPT_WAIT_LIMIT_US: bounded waits of the block form (0 = 4 s)
+    int f_global = 0;             // DGV_OPT_FGLOBAL: 1 = CUDA-core kernels gather f from global memory
     bool tc_autotune = true;      // DGV_OPT_TCAUTOTUNE: tune tiles per CTA and records per launch
     bool tc_user_launch = false;  // the caller set DGV_OPT_TCTILES or DGV_OPT_TCSETMB: no tuning
     std::map<int, std::pair<int, int>> tc_tuned;  // per batch class: (tiles per CTA, MB per launch)
@@ -176,6 +180,14 @@ int set_err(Ctx *c, int code, const std::string &msg);
     } while (0)
 
 int ensure_buffer(Ctx *c, double **p, size_t *have, size_t need_bytes);
+// local-major copies f[v][l*Nc + cell] of nvdf VDFs (FP32 or FP64) in the
+// context's buffer, for the CUDA-core kernels that gather f from global memory
+int f_local_major(Ctx *c, const double *d_f, int nvdf, bool f32, const void **out);
+// the limit of the kernels' bounded waits (DGV_OPT_WAIT_LIMIT_US, else 4 s)
+inline unsigned long long wait_limit_ns(const Ctx *c)
+{
+    return c->wait_limit_us > 0 ? (unsigned long long)c->wait_limit_us * 1000ULL : 4000000000ULL;
+}
 // *dev = true for memory of c's device (or managed), false for host memory;
 // DGV_EINVAL for device memory of another GPU
 int classify_ptr(Ctx *c, const void *p, bool *dev);

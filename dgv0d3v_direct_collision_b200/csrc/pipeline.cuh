@@ -5,8 +5,9 @@
 // contiguous run of rows per stage, completion counted on an mbarrier); the
 // consumer warps wait on a stage's "full" barrier, compute, and arrive on its
 // "empty" barrier so the producer can refill it.  Every wait is bounded: after
-// WAIT_LIMIT polls the waiter raises the kernel's error flag and gives up, so
-// a logic error ends the kernel with a status instead of hanging the GPU.
+// a limit of device time (WAIT_LIMIT_NS unless the context sets another) the
+// waiter raises the kernel's error flag and gives up, so a logic error ends the
+// kernel with a status instead of hanging the GPU.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -106,18 +107,6 @@ struct StageHdr {
 
 // Does the valid output-cell box of a block meet the linear cell range
 // [d0, d1)?  Conservative: compares the linear extent of the box.
-// Producer side of the pipeline (run by one thread): streams, in block order,
-// the rows of every block in [b0, b1) whose box meets the cell range [d0, d1),
-// at most sp pairs per stage, then posts an end-of-stream header.  On the
-// normal path the consumers wait on every stage, so nothing is left in flight
-// when they finish.  If a wait gives up, the producer stops issuing and waits
-// (bounded) for the copies it already issued, so no copy can land in the
-// shared memory of a CTA that has exited.
-template <typename BlockT>
-__device__ __forceinline__ void produce_rows(const BlockT *blk, int b0, int b1, int Mv, int Mw, int d0, int d1,
-                                             const char *rows, int rowb, unsigned char *stages, int sp, int nst,
-                                             StageHdr *hdr, uint64_t *full, uint64_t *empty, int *err);
-
 __device__ __forceinline__ bool box_meets_range(const signed char *lo, const signed char *hi, int Mv, int Mw, int d0,
                                                 int d1)
 {
@@ -126,39 +115,69 @@ __device__ __forceinline__ bool box_meets_range(const signed char *lo, const sig
     return a < d1 && b >= d0;
 }
 
-}  // namespace dgv
-
-namespace dgv {
-
+// Producer side of the pipeline, run by all 32 lanes of one warp: streams, in
+// block order, the rows of every block in [b0, b1) whose box meets the cell
+// range [d0, d1), at most sp pairs per stage, then posts an end-of-stream
+// header.  The lanes test 32 blocks at a time (a CTA's chunk can hold millions
+// of one-pair blocks, e.g. on grids of one node per cell, of which its slice of
+// output cells meets few); lane 0 waits on the stages and issues the copies.
+// On the normal path the consumers wait on every stage, so nothing is left in
+// flight when they finish.  If a wait gives up, the producer stops issuing and
+// waits (bounded) for the copies it already issued, so no copy can land in the
+// shared memory of a CTA that has exited.
 template <typename BlockT>
 __device__ __forceinline__ void produce_rows(const BlockT *blk, int b0, int b1, int Mv, int Mw, int d0, int d1,
                                              const char *rows, int rowb, unsigned char *stages, int sp, int nst,
-                                             StageHdr *hdr, uint64_t *full, uint64_t *empty, int *err)
+                                             StageHdr *hdr, uint64_t *full, uint64_t *empty, int *err,
+                                             unsigned long long wait_ns)
 {
     const size_t stage_bytes = (size_t)sp * rowb;
-    int it = 0;
-    for (int b = b0; b < b1; ++b) {
-        const BlockT bi = blk[b];
-        if (!box_meets_range(bi.lo, bi.hi, Mv, Mw, d0, d1)) continue;
-        for (int off = 0; off < bi.count; off += sp) {
-            const int n = min(sp, bi.count - off), s = it % nst;
-            if (!mbar_wait(&empty[s], ((it / nst) & 1) ^ 1, err)) goto drain;
-            hdr[s] = StageHdr{b, off, n, 0};
-            mbar_arrive_expect_tx(&full[s], (uint32_t)(n * rowb));
-            bulk_g2s(stages + s * stage_bytes, rows + (size_t)(bi.start + off) * rowb, (uint32_t)(n * rowb), &full[s]);
-            it++;
+    const int lane = threadIdx.x & 31;
+    int it = 0;  // stages issued (lane 0)
+    bool ok = true;
+    for (int base = b0; base < b1 && ok; base += 32) {
+        const int b = base + lane;
+        bool meet = false;
+        long long start = 0;
+        int count = 0;
+        if (b < b1) {
+            const BlockT bi = blk[b];
+            meet = box_meets_range(bi.lo, bi.hi, Mv, Mw, d0, d1);
+            start = bi.start;
+            count = bi.count;
+        }
+        unsigned m = __ballot_sync(0xffffffffu, meet);
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const long long st = __shfl_sync(0xffffffffu, start, j);
+            const int cnt = __shfl_sync(0xffffffffu, count, j), bj = base + j;
+            if (lane == 0) {
+                for (int off = 0; off < cnt; off += sp) {
+                    const int n = min(sp, cnt - off), s = it % nst;
+                    if (!mbar_wait(&empty[s], ((it / nst) & 1) ^ 1, err, wait_ns)) { ok = false; break; }
+                    hdr[s] = StageHdr{bj, off, n, 0};
+                    mbar_arrive_expect_tx(&full[s], (uint32_t)(n * rowb));
+                    bulk_g2s(stages + s * stage_bytes, rows + (size_t)(st + off) * rowb, (uint32_t)(n * rowb),
+                             &full[s]);
+                    it++;
+                }
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
         }
     }
-    {
+    if (lane != 0) return;
+    if (ok) {
         const int s = it % nst;
-        if (!mbar_wait(&empty[s], ((it / nst) & 1) ^ 1, err)) goto drain;
-        hdr[s] = StageHdr{-1, 0, 0, 0};
-        mbar_arrive(&full[s]);
+        if (mbar_wait(&empty[s], ((it / nst) & 1) ^ 1, err, wait_ns)) {
+            hdr[s] = StageHdr{-1, 0, 0, 0};
+            mbar_arrive(&full[s]);
+            return;
+        }
     }
-    return;
-drain:
     // the most recent use of each slot is the one still possibly in flight
-    for (int j = it > nst ? it - nst : 0; j < it; j++) mbar_wait(&full[j % nst], (j / nst) & 1, err);
+    for (int j = it > nst ? it - nst : 0; j < it; j++) mbar_wait(&full[j % nst], (j / nst) & 1, err, wait_ns);
 }
 
 }  // namespace dgv

@@ -165,6 +165,13 @@ class DGVSolver:
         """Block form: megabytes of block records per kernel launch."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCSETMB, int(mb)))
 
+    def set_f_global(self, on: bool):
+        """CUDA-core kernels gather f from a local-major copy in global memory
+        instead of staging it in shared memory (DGV_OPT_FGLOBAL; grids whose f
+        does not fit in shared memory use it in any case)."""
+        from ._lib import DGV_OPT_FGLOBAL
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_FGLOBAL, int(on)))
+
     def set_kernel_timing(self, on: bool):
         """Time the collision kernel's launches with CUDA events on the
         context stream (read back with kernel_stats)."""

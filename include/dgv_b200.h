@@ -65,15 +65,23 @@ extern "C" {
 #define DGV_OPT_TCSETMB 6  /* block form: MB of block records per kernel     */
                            /* launch (default 48; a launch's records are read */
                            /* by all its CTAs, so they should stay in L2)     */
-#define DGV_OPT_WAIT_LIMIT_US 7  /* block form: microseconds after which a    */
-                                 /* bounded device wait gives up (0 = 4 s);   */
-                                 /* the call then returns DGV_ETIMEOUT        */
+#define DGV_OPT_WAIT_LIMIT_US 7  /* microseconds after which a bounded wait   */
+                                 /* of a collision kernel (block form, FP64,  */
+                                 /* FP32-compensated, mixed terms, adjoint)   */
+                                 /* gives up (0 = 4 s); the call then returns */
+                                 /* DGV_ETIMEOUT                              */
 #define DGV_OPT_TCAUTOTUNE 9      /* block form: 1 (default) = on the first    */
                                  /* evaluation of each batch class, time VDF  */
                                  /* tiles per CTA x records per launch and    */
                                  /* keep the fastest; 0 = the options' values */
                                  /* (setting DGV_OPT_TCTILES or _TCSETMB also */
                                  /* switches the tuning off)                  */
+#define DGV_OPT_FGLOBAL 10        /* CUDA-core kernels (FP64, FP32-compensated, */
+                                 /* mixed terms, FP64 adjoint): 0 (default) = */
+                                 /* f of a VDF staged in shared memory when   */
+                                 /* it fits, else gathered from a local-major */
+                                 /* copy in global memory (L1/L2); 1 = always */
+                                 /* the global copy                           */
 #define DGV_OPT_TEST_WITHHOLD 8  /* 1: test of the bounded waits: the next    */
                                  /* block-form call leaves one of its copies  */
                                  /* unissued, so its waits run out and it     */
