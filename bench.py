@@ -259,16 +259,16 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def load_profile_traffic(form: int, set_mb: int = 0):
+def load_profile_traffic(form: int, set_mb: int = 0, persistent: int = 0):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/k_collide_tc2_27cubed_b256.json for the block form, per
-    MB of block records per launch; k_collide_tc_27cubed_b256.json for the
-    chunk form), or None."""
+    MB of block records per set, "<MB>p" for one persistent launch per
+    evaluation; k_collide_tc_27cubed_b256.json for the chunk form), or None."""
     name = "k_collide_tc2_27cubed_b256.json" if form == 2 else "k_collide_tc_27cubed_b256.json"
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", name)))
         if "dram_bytes_per_launch_by_set_mb" in d:
-            v = d["dram_bytes_per_launch_by_set_mb"].get(str(set_mb))
+            v = d["dram_bytes_per_launch_by_set_mb"].get(str(set_mb) + ("p" if persistent else ""))
             return (float(v) if v is not None else None), d.get("note", "")
         return float(d["dram_bytes_per_launch"]), d.get("note", "")
     except Exception:
@@ -289,6 +289,8 @@ def run_ours(args, world, rank, local):
         solver.set_tc_tiles_per_cta(args.tc_tiles)
     if args.tc_set_mb:
         solver.set_tc_set_mb(args.tc_set_mb)
+    if args.tc_persistent >= 0:
+        solver.set_tc_persistent(bool(args.tc_persistent))
     t = time.perf_counter()
     solver.generate_synthetic_A(seed=SEED_A, support=1)
     t_gen = time.perf_counter() - t
@@ -308,10 +310,12 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
     t_prep = time.perf_counter() - t
     plan = solver.tc_plan(BATCH)  # the records and lists exist now
-    from dgv0d3v_direct_collision_b200._lib import DGV_OPT_TCSETMB, DGV_OPT_TCTILES
+    from dgv0d3v_direct_collision_b200._lib import DGV_OPT_TCPERSIST, DGV_OPT_TCSETMB, DGV_OPT_TCTILES
     tc_launch = {"tiles_per_cta": solver.get_option(DGV_OPT_TCTILES),
                  "set_mb": solver.get_option(DGV_OPT_TCSETMB),
-                 "chosen_by": "the library's autotuner" if not (args.tc_tiles or args.tc_set_mb) else "options"}
+                 "persistent": solver.get_option(DGV_OPT_TCPERSIST),
+                 "chosen_by": ("the library's autotuner" if not (args.tc_tiles or args.tc_set_mb or args.tc_persistent >= 0)
+                               else "options")}
     solver.set_kernel_timing(True)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup - 1):
@@ -421,7 +425,7 @@ def run_ours(args, world, rank, local):
     # FLOPs the MMAs issue per launch (dense tiles, three split products) over the same time
     issued = plan["tensor_flop"] / max(plan["launches"], 1) / (k_ms_launch / 1000.0) / 1e12
     form = solver.tc_form
-    traffic, tnote = load_profile_traffic(form, tc_launch["set_mb"])
+    traffic, tnote = load_profile_traffic(form, tc_launch["set_mb"], tc_launch["persistent"])
     kname = "k_collide_tc2<128,27>" if form == 2 else "k_collide_tc<128>"
     knote = ("algorithmic FLOPs = 3 per record-shift (A*f*f + add) x VDFs; the block form computes "
              "G = f(c2) W per cell-pair block on the tensor core (dense W: 27 x 729 per block, 3 fp16 "
@@ -497,6 +501,8 @@ def run_mixed(args):
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
+        for sol, _, _ in members:  # launches of the timed steps only
+            sol.kernel_stats(reset=True)
         with ClockSampler(0) as clk:
             e0.record(stream)
             for _ in range(args.steps):
@@ -514,9 +520,9 @@ def run_mixed(args):
             sol.EvalCollisionPeriodicAPlus_DGV(f, q, precision="tc")
 
     for sol, _, _ in members:
-        sol.kernel_stats(reset=True)
+        sol.set_kernel_timing(True)
     ms_g, clk = timed(group)
-    launches = sum(m[0].kernel_stats(reset=True)["all_launches"] for m in members)
+    launches = sum(m[0].kernel_stats(reset=True)["all_launches"] for m in members) / args.steps
     q_group = [m[2].clone() for m in members]
     ms_s, _ = timed(separate)
     same = all(torch.equal(a, m[2]) for a, m in zip(q_group, members))
@@ -528,9 +534,12 @@ def run_mixed(args):
         "data": "synthetic",
         "config": {"workload": "768 VDFs on s=3,M=7,[-6,6]^3 + 256 VDFs on s=3,M=5,[-6,6]^3, tensor-core path",
                    "A": [m[0].A_info() for m in members],
-                   "l2": "inputs larger than L2: A chunk records of both grids streamed every step"},
+                   "l2": "inputs larger than L2: the block records of both grids (~4 GB) are streamed every step"},
         "separate_calls_ms_per_step": ms_s, "group_over_separate": ms_s / ms_g,
-        "group_equals_separate": bool(same), "gpu_launches": int(launches), "clocks": clk}))
+        "group_equals_separate": bool(same), "gpu_launches": int(round(launches)),
+        "gpu_launches_note": "kernel launches per step inside the one graph launch (preparation and final "
+                             "kernels per grid, one persistent collision kernel for both grids)",
+        "clocks": clk}))
 
 
 def run_trajectory(args):
@@ -605,6 +614,8 @@ def run_profile_case(case: str, args=None):
         s.set_tc_set_mb(args.tc_set_mb)
     if args is not None and args.tc_tiles:
         s.set_tc_tiles_per_cta(args.tc_tiles)
+    if args is not None and args.tc_persistent >= 0:
+        s.set_tc_persistent(bool(args.tc_persistent))
     if prec not in ("tc", "vjptc"):
         s.set_nchunks(296)
     nb = BATCH if prec in ("tc", "vjptc") else 1
@@ -652,6 +663,9 @@ def main():
                     help="timed tensor-core VJP evaluations of the batch (0 = skip the adjoint)")
     ap.add_argument("--tc-set-mb", type=int, default=0,
                     help="block form: MB of block records per launch (0 = the library default)")
+    ap.add_argument("--tc-persistent", type=int, default=-1, choices=[-1, 0, 1],
+                    help="block form: 1 = one persistent launch per evaluation, 0 = one launch per set "
+                         "(-1 = the library's choice)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

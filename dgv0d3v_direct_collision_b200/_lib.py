@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libdgv_b200.so")
 DGV_OK, DGV_EINVAL, DGV_ERANGE, DGV_ECUDA, DGV_ETIMEOUT, DGV_ENOMEM, DGV_ESTATE, DGV_EUNSUP = range(8)
 DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC = 0, 1, 2
 DGV_OPT_PROJECT, DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM, DGV_OPT_TCTILES, DGV_OPT_TCSETMB = 1, 2, 3, 4, 5, 6
-DGV_OPT_WAIT_LIMIT_US, DGV_OPT_TEST_WITHHOLD, DGV_OPT_TCAUTOTUNE, DGV_OPT_FGLOBAL = 7, 8, 9, 10
+DGV_OPT_WAIT_LIMIT_US, DGV_OPT_TEST_WITHHOLD, DGV_OPT_TCAUTOTUNE, DGV_OPT_FGLOBAL, DGV_OPT_TCPERSIST = 7, 8, 9, 10, 11
 
 STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4: "DGV_ETIMEOUT",
                 5: "DGV_ENOMEM", 6: "DGV_ESTATE", 7: "DGV_EUNSUP"}

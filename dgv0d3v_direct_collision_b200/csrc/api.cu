@@ -165,7 +165,7 @@ static void destroy_ctx(Ctx *c)
     free_ktimers(c);
     free_layout(c->lay);
     double *bufs[] = {c->d_nu, c->d_nv, c->d_nw, c->d_nwt, c->d_partial, c->d_in, c->d_out, c->d_red, c->d_fm,
-                      c->d_tcF, c->d_tcQ, c->d_glm, c->d_fg, c->d_fmn, c->d_dfr, c->d_rgt};
+                      c->d_tcF, c->d_tcQ, c->d_glm, c->d_fg, c->d_tc2done, c->d_fmn, c->d_dfr, c->d_rgt};
     for (double *p : bufs)
         if (p) cudaFree(p);
     for (double *p : c->d_tmp)
@@ -356,6 +356,12 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
     case DGV_OPT_TEST_WITHHOLD:
         ctx->c.test_withhold = value != 0;
         return DGV_OK;
+    case DGV_OPT_TCPERSIST:
+        if (value != 0 && value != 1) return set_err(&ctx->c, DGV_EINVAL, "persistent launches: 0 or 1");
+        ctx->c.tc_persistent = (int)value;
+        ctx->c.tc_user_launch = true;
+        release_graphs(&ctx->c);
+        return DGV_OK;
     case DGV_OPT_FGLOBAL:
         if (value != 0 && value != 1) return set_err(&ctx->c, DGV_EINVAL, "f placement must be 0 (auto) or 1 (global)");
         ctx->c.f_global = (int)value;
@@ -366,9 +372,11 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value)
         ctx->c.tc_autotune = value != 0;
         if (!value) {  // back to the fixed defaults (unless the caller set them)
             ctx->c.tc_tuned.clear();
+            ctx->c.tc_tuned_adj.clear();
             if (!ctx->c.tc_user_launch) {
                 ctx->c.tc_tiles_per_cta = 2;
                 ctx->c.tc_set_mb = 48;
+                ctx->c.tc_persistent = 0;
             }
         }
         release_graphs(&ctx->c);
@@ -393,6 +401,7 @@ int dgv_get_option(dgv_ctx *ctx, int option, int64_t *value)
     case DGV_OPT_TCAUTOTUNE: *value = c.tc_autotune ? 1 : 0; return DGV_OK;
     case DGV_OPT_TEST_WITHHOLD: *value = c.test_withhold ? 1 : 0; return DGV_OK;
     case DGV_OPT_FGLOBAL: *value = c.f_global; return DGV_OK;
+    case DGV_OPT_TCPERSIST: *value = c.tc_persistent; return DGV_OK;
     default: return set_err(&ctx->c, DGV_EINVAL, "unknown option");
     }
 }

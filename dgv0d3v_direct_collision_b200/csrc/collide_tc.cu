@@ -919,18 +919,106 @@ struct Tc2Args {
     const unsigned char *F16;  // [nbt][hi, lo][Nc][VB x 32 tile]
     const unsigned char *W;    // block records
     const unsigned char *W2;   // adjoint: the records of its pass to the c2 side (items with 1 << 30)
-    const TcItem *items;       // work lists of this launch (chunk0 = first record group, | 1 << 30 for W2)
-    const int *item_start;     // [ntiles + 1]
-    const int *tile_of;        // row-tile index in launch order
+    const TcItem *items;       // work lists (chunk0 = first record group, | 1 << 30 for W2)
+    const int *item_start;     // per block set: [ng + 1]
+    const int *tile_of;        // per block set: row-tile index in work order [ng]
     double *qacc;              // [(D*P+p)*NV + vdf]
     const double *inv_scale;   // [NV]
     int *err;
+    int *done;   // persistent launches: per (row tile, VDF-tile pair, epilogue warp) the sets added to qacc
     int Nc, ccell, NV, nvdf, nbt, nbp;
     int tpc;     // VDF tiles per CTA (1 or 2)
+    int ng;      // row tiles
+};
+
+constexpr int T2_MAXG = 4;  // grids of one launch (mixed-grid batches)
+
+// One launch of the block form.  Its work is a sequence of units, unit
+// ubase[g] + (s*ng + t)*nbp + bp serving, for grid g, block set s, the t-th
+// row tile of that set's order (heaviest first) and the VDF tiles
+// tpc*bp .. tpc*bp + tpc-1.
+//   one launch per block set: CTA b serves unit b;
+//   persistent (one launch for all sets and grids, one CTA per SM): each CTA's
+//   producer takes the next unit from a counter (atomicAdd: units are handed
+//   out in increasing order, balanced like the hardware's CTA dispatch) and
+//   passes it to the MMA thread and the epilogue warps through a two-entry
+//   queue in shared memory; the FP64 sums of a unit go into qacc after those
+//   of the same rows' previous set (per-warp flags in done), so the additions
+//   happen in the same order as with one launch per set and the results are
+//   the same bit for bit.  A unit's predecessor has a smaller index, so it was
+//   handed out earlier to a resident CTA: the waits on the flags end.
+struct Tc2Launch {
+    Tc2Args g[T2_MAXG];
+    int ngrids;
+    int ubase[T2_MAXG + 1];
+    int *counter;  // persistent: the next unit to hand out (starts at 0); nullptr: unit = blockIdx.x
+    int tpcmax;    // persistent: the VDF tiles every unit of the launch holds (the host launches persistent
+                   // kernels only when all units hold the same number)
     int region;  // bytes per VDF tile in an item slot: A hi, A lo, side (FP32), slot header
     unsigned long long wait_ns;  // limit of every bounded wait
     int withhold;  // test of the bounded waits: CTA 0 withholds its first W copy
 };
+
+struct T2Unit {
+    int gi, s, bp, tile, i0, i1, bt0, nb2;
+};
+
+// MG: the launch serves several grids (the unit's grid is looked up); else grid 0
+template <bool MG>
+__device__ __forceinline__ T2Unit t2_unit(const Tc2Launch &L, int u)
+{
+    T2Unit r;
+    r.gi = 0;
+    if constexpr (MG)
+        while (r.gi + 1 < L.ngrids && u >= L.ubase[r.gi + 1]) r.gi++;
+    const Tc2Args &a = L.g[MG ? r.gi : 0];
+    int v = u - L.ubase[r.gi];
+    const int per = a.nbp * a.ng;
+    r.s = v / per;
+    v -= r.s * per;
+    r.bp = v % a.nbp;
+    const int ti = v / a.nbp;
+    r.tile = a.tile_of[(size_t)r.s * a.ng + ti];
+    r.i0 = a.item_start[(size_t)r.s * (a.ng + 1) + ti];
+    r.i1 = a.item_start[(size_t)r.s * (a.ng + 1) + ti + 1];
+    r.bt0 = a.tpc * r.bp;
+    r.nb2 = min(a.tpc, a.nbt - r.bt0);
+    return r;
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// bounded wait until *flag >= target (another CTA's release); like mbar_wait
+// it gives up after limit_ns (raising err) or when err is raised elsewhere
+__device__ __forceinline__ bool flag_wait(const int *flag, int target, int *err, unsigned long long limit_ns)
+{
+    if (ld_acquire_gpu(flag) >= target) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned long long tcheck = t0;
+    while (ld_acquire_gpu(flag) < target) {
+        __nanosleep(256);
+        const unsigned long long t = globaltimer_ns();
+        if (t - t0 > limit_ns) {
+            *(volatile int *)err = 1;
+            return false;
+        }
+        if (t - tcheck > 1000000ULL) {
+            tcheck = t;
+            if (*(volatile int *)err) return false;
+        }
+    }
+    return true;
+}
 
 // MODE 0: Q(f,f), a CTA owns output cells D and an item (block c1, c2) reads
 //         F16 tiles of cells c2 + D and the FP32 side tile of cells c1 + D;
@@ -946,26 +1034,33 @@ struct Tc2Args {
 //         of the mask gets sum_p c(D, p) G[(rank(l), p)].
 // Both modes: an item's nch holds the block's node mask (low 27 bits) and the
 // owner cells it serves (bits 27..30), chunk0 its first record group.
-template <int VB, int P, int MODE>
-__global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
+// The three roles walk the same units and items in the same order; their
+// counters of items, W groups and (group, VDF tile) jobs run on across units.
+template <int VB, int P, int MODE, bool MG>
+__global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_constant__ Tc2Launch L)
 {
     constexpr int NDG = TC_ROWS / VB;
     constexpr int NG = t2_groups(P);
     extern __shared__ __align__(1024) unsigned char smem[];
+    const int region = L.region;
     unsigned char *wring = smem;                      // T2_NSTW x T2_GREC
     unsigned char *slots = smem + T2_NSTW * T2_GREC;  // 2 item slots x 2 VDF tiles x region
-    uint64_t *bars = reinterpret_cast<uint64_t *>(slots + 4 * a.region);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(slots + 4 * region);
     uint64_t *w_full = bars, *w_empty = bars + T2_NSTW;
     uint64_t *s_full = w_empty + T2_NSTW, *s_empty = s_full + 2;
     uint64_t *c_full = s_empty + 2, *c_empty = c_full + 2;
     uint64_t *drain = c_empty + 4;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    uint64_t *uq_full = drain + 1, *uq_empty = uq_full + 2;  // unit queue
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(uq_empty + 2);
+    volatile int *uq = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bp = blockIdx.x % a.nbp, ti = blockIdx.x / a.nbp;
-    const int bt0 = a.tpc * bp, nb2 = min(a.tpc, a.nbt - bt0);
-    const int D0 = a.tile_of[ti] * NDG;
-    const int i0 = a.item_start[ti], i1 = a.item_start[ti + 1];
+    const int total = L.ubase[L.ngrids];
+    int *const err0 = L.g[0].err;
+    // VDF tiles this CTA's units hold: its one unit's (one launch per set), or
+    // the launch's (persistent: the same in every unit); the epilogue warps of
+    // the other tile leave at once, as if the CTA had been launched without them
+    const int nbw = L.counter ? L.tpcmax : (blockIdx.x < (unsigned)total ? t2_unit<MG>(L, blockIdx.x).nb2 : 1);
     if (threadIdx.x == 0) {
         for (int s = 0; s < T2_NSTW; s++) {
             mbar_init(&w_full[s], 1);
@@ -973,13 +1068,17 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
         }
         for (int s = 0; s < 2; s++) {
             mbar_init(&s_full[s], 1);
-            mbar_init(&s_empty[s], 1 + 4 * nb2);  // the MMA commit + the epilogue warps
+            mbar_init(&s_empty[s], 1 + 4 * nbw);  // the MMA commit + the epilogue warps of the CTA's tiles
         }
         for (int s = 0; s < 2; s++) {
             mbar_init(&c_full[s], 1);
-            mbar_init(&c_empty[s], 4);
+            mbar_init(&c_empty[s], 4);  // the epilogue warps of the job's tile
         }
         mbar_init(drain, 1);
+        for (int s = 0; s < 2; s++) {
+            mbar_init(&uq_full[s], 1);
+            mbar_init(&uq_empty[s], 1 + 4 * nbw);  // the MMA thread + the epilogue warps of the CTA's tiles
+        }
         fence_mbar_init();
     }
     if (warp == 1) {
@@ -995,7 +1094,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
     // grid, so rows of such cells read what the slot held before -- zeros or
     // finite values of earlier items, which the zero side factors of rows an
     // item does not serve turn into exact zeros
-    for (int t = threadIdx.x; t < a.region / 4; t += blockDim.x)
+    for (int t = threadIdx.x; t < region / 4; t += blockDim.x)  // 4 slots of `region` bytes, 16 B per store
         reinterpret_cast<uint4 *>(slots)[t] = make_uint4(0u, 0u, 0u, 0u);
     fence_async_shared();  // visible to the tensor core and ordered before the copies
     if (warp >= 2) {
@@ -1018,66 +1117,86 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             int q = 0, gw = 0;
             bool ok = true;
             const size_t tile = (size_t)VB * T2_K * 2;
-            for (int it = i0; it < i1 && ok; it++) {
-                const TcItem e = a.items[it];
-                const int s = q & 1;
-                if (!mbar_wait(&s_empty[s], ((q >> 1) & 1) ^ 1, a.err, a.wait_ns)) { ok = false; break; }
-                // f of cells c1 + D - ccell (FP32) and c2 + D - ccell (fp16
-                // tiles), D in the row tile, clipped to the grid
-                const int cs1 = e.c1 + D0 - a.ccell, cs2 = e.c2 + D0 - a.ccell;
-                const int lo1 = max(cs1, 0), hi1 = min(cs1 + NDG, a.Nc);
-                const int lo2 = max(cs2, 0), hi2 = min(cs2 + NDG, a.Nc);
-                {
-                    int *hd = reinterpret_cast<int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE +
-                                                      NDG * P * VB * 4);
-                    const unsigned msk = (unsigned)e.nch & 0x7ffffffu;
-                    int k = 0;
-                    for (int l = 0; l < P; l++)
-                        if ((msk >> l) & 1u) hd[1 + k++] = l * VB;
-                    hd[0] = k * P;
-                    for (; k < P; k++) hd[1 + k] = -1;
-                    hd[1 + P] = e.nch;
+            for (int k = 0; ok; k++) {
+                int u = k == 0 ? (int)blockIdx.x : total;
+                if (L.counter) {
+                    // hand the next unit to the other roles (a unit >= total ends them)
+                    const int slot = k & 1;
+                    if (!mbar_wait(&uq_empty[slot], ((k >> 1) & 1) ^ 1, err0, L.wait_ns)) { ok = false; break; }
+                    u = atomicAdd(L.counter, 1);
+                    uq[slot] = u;
+                    mbar_arrive(&uq_full[slot]);
                 }
-                uint32_t tx = 0;
-                if (hi1 > lo1) tx += (uint32_t)(nb2 * (hi1 - lo1) * P * VB * 4);
-                if (hi2 > lo2) tx += (uint32_t)(nb2 * 2 * (hi2 - lo2) * tile);
-                if (tx) {
-                    mbar_arrive_expect_tx(&s_full[s], tx);
-                    for (int j = 0; j < nb2; j++) {
-                        const int bt = bt0 + j;
-                        unsigned char *reg = slots + (size_t)(2 * s + j) * a.region;
-                        if (hi2 > lo2) {
-                            const unsigned char *src = a.F16 + ((size_t)(2 * bt) * a.Nc + lo2) * tile;
-                            const uint32_t nb = (uint32_t)((hi2 - lo2) * tile);
-                            bulk_g2s(reg + (lo2 - cs2) * tile, src, nb, &s_full[s]);
-                            bulk_g2s(reg + T2_ATILE + (lo2 - cs2) * tile, src + (size_t)a.Nc * tile, nb, &s_full[s]);
-                        }
-                        if (hi1 > lo1)
-                            bulk_g2s(reg + 2 * T2_ATILE + (size_t)(lo1 - cs1) * P * VB * 4,
-                                     a.F + ((size_t)bt * a.Nc + lo1) * P * VB, (uint32_t)((hi1 - lo1) * P * VB * 4),
-                                     &s_full[s]);
+                if (u >= total) break;
+                const T2Unit un = t2_unit<MG>(L, u);
+                const Tc2Args &a = L.g[MG ? un.gi : 0];
+                const int D0 = un.tile * NDG;
+                for (int it = un.i0; it < un.i1; it++) {
+                    const TcItem e = a.items[it];
+                    const int s = q & 1;
+                    if (!mbar_wait(&s_empty[s], ((q >> 1) & 1) ^ 1, a.err, L.wait_ns)) { ok = false; break; }
+                    // f of cells c1 + D - ccell (FP32) and c2 + D - ccell (fp16
+                    // tiles), D in the row tile, clipped to the grid
+                    const int cs1 = e.c1 + D0 - a.ccell, cs2 = e.c2 + D0 - a.ccell;
+                    const int lo1 = max(cs1, 0), hi1 = min(cs1 + NDG, a.Nc);
+                    const int lo2 = max(cs2, 0), hi2 = min(cs2 + NDG, a.Nc);
+                    {
+                        int *hd = reinterpret_cast<int *>(slots + (size_t)(2 * s) * region + 2 * T2_ATILE +
+                                                          NDG * P * VB * 4);
+                        const unsigned msk = (unsigned)e.nch & 0x7ffffffu;
+                        int k = 0;
+                        for (int l = 0; l < P; l++)
+                            if ((msk >> l) & 1u) hd[1 + k++] = l * VB;
+                        hd[0] = k * P;
+                        for (; k < P; k++) hd[1 + k] = -1;
+                        hd[1 + P] = e.nch;
                     }
-                } else {
-                    mbar_arrive(&s_full[s]);
-                }
-                q++;
-                // the item's compacted record: groups from chunk0 & 0x3fffffff
-                // of W, or of W2 for the adjoint's pass to the c2 side
-                const int ngb = t2_item_groups<P>(e.nch);
-                const unsigned char *wrec =
-                    ((MODE == 1 && (e.chunk0 >> 30)) ? a.W2 : a.W) + (size_t)(e.chunk0 & 0x3fffffff) * T2_GREC;
-                for (int g = 0; g < ngb; g++, gw++) {
-                    const int st = gw % T2_NSTW;
-                    if (!mbar_wait(&w_empty[st], ((gw / T2_NSTW) & 1) ^ 1, a.err, a.wait_ns)) { ok = false; break; }
-                    if (a.withhold && blockIdx.x == 0 && gw == 0) continue;  // the stage nothing completes
-                    mbar_arrive_expect_tx(&w_full[st], T2_GREC);
-                    bulk_g2s(wring + st * T2_GREC, wrec + (size_t)g * T2_GREC, T2_GREC, &w_full[st]);
+                    uint32_t tx = 0;
+                    if (hi1 > lo1) tx += (uint32_t)(un.nb2 * (hi1 - lo1) * P * VB * 4);
+                    if (hi2 > lo2) tx += (uint32_t)(un.nb2 * 2 * (hi2 - lo2) * tile);
+                    if (tx) {
+                        mbar_arrive_expect_tx(&s_full[s], tx);
+                        for (int j = 0; j < un.nb2; j++) {
+                            const int bt = un.bt0 + j;
+                            unsigned char *reg = slots + (size_t)(2 * s + j) * region;
+                            if (hi2 > lo2) {
+                                const unsigned char *src = a.F16 + ((size_t)(2 * bt) * a.Nc + lo2) * tile;
+                                const uint32_t nb = (uint32_t)((hi2 - lo2) * tile);
+                                bulk_g2s(reg + (lo2 - cs2) * tile, src, nb, &s_full[s]);
+                                bulk_g2s(reg + T2_ATILE + (lo2 - cs2) * tile, src + (size_t)a.Nc * tile, nb,
+                                         &s_full[s]);
+                            }
+                            if (hi1 > lo1)
+                                bulk_g2s(reg + 2 * T2_ATILE + (size_t)(lo1 - cs1) * P * VB * 4,
+                                         a.F + ((size_t)bt * a.Nc + lo1) * P * VB, (uint32_t)((hi1 - lo1) * P * VB * 4),
+                                         &s_full[s]);
+                        }
+                    } else {
+                        mbar_arrive(&s_full[s]);
+                    }
+                    q++;
+                    // the item's compacted record: groups from chunk0 & 0x3fffffff
+                    // of W, or of W2 for the adjoint's pass to the c2 side
+                    const int ngb = t2_item_groups<P>(e.nch);
+                    const unsigned char *wrec =
+                        ((MODE == 1 && (e.chunk0 >> 30)) ? a.W2 : a.W) + (size_t)(e.chunk0 & 0x3fffffff) * T2_GREC;
+                    for (int g = 0; g < ngb; g++, gw++) {
+                        const int st = gw % T2_NSTW;
+                        if (!mbar_wait(&w_empty[st], ((gw / T2_NSTW) & 1) ^ 1, a.err, L.wait_ns)) {
+                            ok = false;
+                            break;
+                        }
+                        if (L.withhold && blockIdx.x == 0 && gw == 0) continue;  // the stage nothing completes
+                        mbar_arrive_expect_tx(&w_full[st], T2_GREC);
+                        bulk_g2s(wring + st * T2_GREC, wrec + (size_t)g * T2_GREC, T2_GREC, &w_full[st]);
+                    }
+                    if (!ok) break;
                 }
             }
             if (!ok) {  // let the copies already issued land
                 for (int j = gw > T2_NSTW ? gw - T2_NSTW : 0; j < gw; j++)
-                    mbar_wait(&w_full[j % T2_NSTW], (j / T2_NSTW) & 1, a.err, a.wait_ns);
-                for (int j = q > 2 ? q - 2 : 0; j < q; j++) mbar_wait(&s_full[j & 1], (j >> 1) & 1, a.err, a.wait_ns);
+                    mbar_wait(&w_full[j % T2_NSTW], (j / T2_NSTW) & 1, err0, L.wait_ns);
+                for (int j = q > 2 ? q - 2 : 0; j < q; j++) mbar_wait(&s_full[j & 1], (j >> 1) & 1, err0, L.wait_ns);
             }
         }
         __syncwarp();
@@ -1090,158 +1209,205 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
             const uint32_t idesc = (1u << 4) | ((uint32_t)(T2_N >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             int q = 0, gw = 0, J = 0;
             bool ok = true;
-            for (int it = i0; it < i1 && ok; it++) {
-                const int s = q & 1;
-                if (!mbar_wait(&s_full[s], (q >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
-                const int ncol = *reinterpret_cast<const int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE +
-                                                                 NDG * P * VB * 4);
-                const int ngb = (ncol + T2_N - 1) / T2_N;
-                const int nlast = ((ncol - (ngb - 1) * T2_N) + 15) / 16 * 16;
-                const uint32_t idesc_last = (1u << 4) | ((uint32_t)(nlast >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
-                for (int g = 0; g < ngb && ok; g++, gw++) {
-                    const int st = gw % T2_NSTW;
-                    if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, a.err, a.wait_ns)) { ok = false; break; }
-                    const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
-                    const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
-                    const uint32_t id = g == ngb - 1 ? idesc_last : idesc;
-                    for (int j = 0; j < nb2; j++, J++) {
-                        const int cs = J & 1;
-                        if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, a.err, a.wait_ns)) { ok = false; break; }
-                        tc_fence_after();
-                        unsigned char *reg = slots + (size_t)(2 * s + j) * a.region;
-                        const uint64_t dAh = umma_desc(smem_u32(reg), 128, 512);
-                        const uint64_t dAl = umma_desc(smem_u32(reg + T2_ATILE), 128, 512);
-                        const uint32_t dacc = tmem + (uint32_t)(cs * T2_N);
+            for (int k = 0; ok; k++) {
+                int u = k == 0 ? (int)blockIdx.x : total;
+                if (L.counter) {
+                    const int slot = k & 1;
+                    if (!mbar_wait(&uq_full[slot], (k >> 1) & 1, err0, L.wait_ns)) { ok = false; break; }
+                    u = uq[slot];
+                    mbar_arrive(&uq_empty[slot]);
+                }
+                if (u >= total) break;
+                const T2Unit un = t2_unit<MG>(L, u);
+                int *const err = L.g[MG ? un.gi : 0].err;
+                for (int it = un.i0; it < un.i1 && ok; it++) {
+                    const int s = q & 1;
+                    if (!mbar_wait(&s_full[s], (q >> 1) & 1, err, L.wait_ns)) { ok = false; break; }
+                    const int ncol = *reinterpret_cast<const int *>(slots + (size_t)(2 * s) * region + 2 * T2_ATILE +
+                                                                     NDG * P * VB * 4);
+                    const int ngb = (ncol + T2_N - 1) / T2_N;
+                    const int nlast = ((ncol - (ngb - 1) * T2_N) + 15) / 16 * 16;
+                    const uint32_t idesc_last =
+                        (1u << 4) | ((uint32_t)(nlast >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+                    for (int g = 0; g < ngb && ok; g++, gw++) {
+                        const int st = gw % T2_NSTW;
+                        if (!mbar_wait(&w_full[st], (gw / T2_NSTW) & 1, err, L.wait_ns)) { ok = false; break; }
+                        const uint64_t dWh = umma_desc(smem_u32(wring + st * T2_GREC), 128, 512);
+                        const uint64_t dWl = umma_desc(smem_u32(wring + st * T2_GREC + T2_TILE), 128, 512);
+                        const uint32_t id = g == ngb - 1 ? idesc_last : idesc;
+                        for (int j = 0; j < un.nb2; j++, J++) {
+                            const int cs = J & 1;
+                            if (!mbar_wait(&c_empty[cs], ((J >> 1) & 1) ^ 1, err, L.wait_ns)) { ok = false; break; }
+                            tc_fence_after();
+                            unsigned char *reg = slots + (size_t)(2 * s + j) * region;
+                            const uint64_t dAh = umma_desc(smem_u32(reg), 128, 512);
+                            const uint64_t dAl = umma_desc(smem_u32(reg + T2_ATILE), 128, 512);
+                            const uint32_t dacc = tmem + (uint32_t)(cs * T2_N);
 #pragma unroll
-                        for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 256 B along K
-                            umma_f16(dacc, dAh + 16 * t, dWh + 16 * t, id, t ? 1u : 0u);
-                            umma_f16(dacc, dAh + 16 * t, dWl + 16 * t, id, 1u);
-                            umma_f16(dacc, dAl + 16 * t, dWh + 16 * t, id, 1u);
+                            for (int t = 0; t < T2_K / 16; t++) {  // K = 16 per instruction: 256 B along K
+                                umma_f16(dacc, dAh + 16 * t, dWh + 16 * t, id, t ? 1u : 0u);
+                                umma_f16(dacc, dAh + 16 * t, dWl + 16 * t, id, 1u);
+                                umma_f16(dacc, dAl + 16 * t, dWh + 16 * t, id, 1u);
+                            }
+                            umma_commit(&c_full[cs]);
                         }
-                        umma_commit(&c_full[cs]);
+                        if (!ok) break;
+                        umma_commit(&w_empty[st]);
                     }
                     if (!ok) break;
-                    umma_commit(&w_empty[st]);
+                    umma_commit(&s_empty[s]);
+                    q++;
                 }
-                if (!ok) break;
-                umma_commit(&s_empty[s]);
-                q++;
             }
             // every MMA issued so far completes before tensor memory is freed
             umma_commit(drain);
-            mbar_wait(drain, 0, a.err, a.wait_ns);
+            mbar_wait(drain, 0, err0, L.wait_ns);
         }
         __syncwarp();
-    } else if ((warp - 2) / 4 < nb2) {
+    } else if ((warp - 2) / 4 < nbw) {
         // ---------------- epilogue ----------------
+        // warp w serves VDF tile (w-2)/4 of every unit of the CTA
         const int j = (warp - 2) / 4, quarter = warp & 3, r = quarter * 32 + lane;
         const uint32_t tl = tmem + ((uint32_t)(quarter * 32) << 16);
         const int d = r / VB, v = r % VB;
-        float S[P], Cc[P];
-#pragma unroll
-        for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
-        int q = 0, gq = 0;  // items and column groups consumed so far
-        float acc[MODE == 0 ? P : 1];  // MODE 0: the item's FP32 sums
-#pragma unroll
-        for (int p = 0; p < (MODE == 0 ? P : 1); p++) acc[p] = 0.f;
+        int q = 0, Jb = 0;  // items consumed; (group, VDF tile) jobs of the items before
         bool ok = true;
-        for (int it = i0; it < i1 && ok; it++) {
-            const int s = q & 1;
-            if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
-            const float *f1s =
-                reinterpret_cast<const float *>(slots + (size_t)(2 * s + j) * a.region + 2 * T2_ATILE) + d * P * VB + v;
-            const int *hoff =
-                reinterpret_cast<const int *>(slots + (size_t)(2 * s) * a.region + 2 * T2_ATILE + NDG * P * VB * 4) + 1;
-            const int nch = hoff[P];
-            const bool valid = (nch >> (27 + d)) & 1;
-            const unsigned msk = (unsigned)nch & 0x7ffffffu;
-            const int nl = __popc(msk), ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
-            // Columns n = jj*P + p, jj = the rank of a node of the item's mask.
-            // MODE 0: side = f(c1 + D, l1) of the jj-th node l1 (its offset from
-            //         the slot header; 0 past the mask's nodes),
-            //         acc[p] += side * G[n].
-            // MODE 1: side = c(D, p) (all P live), the sum over p of each jj is
-            //         complete after its P consecutive columns and is kept in
-            //         stg[jj] (local memory: its read index is the rank of a
-            //         node); after the item each node l of the mask adds
-            //         stg[rank(l)] into its (sum, correction).
-            float f1[P], stg[MODE == 1 ? P : 1], run[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int l = 0; l < P; l++) {
-                if constexpr (MODE == 1) {
-                    f1[l] = f1s[l * VB];
-                } else {
-                    // loaded before the column loop (the TMEM waits order all
-                    // shared-memory loads, so loads inside it would stall); a
-                    // row the item does not serve gets zero factors, so its
-                    // columns add exact zeros
-                    const int o = hoff[l];
-                    f1[l] = (valid && o >= 0) ? f1s[o] : 0.f;
-                }
+        for (int k = 0; ok; k++) {
+            int u = k == 0 ? (int)blockIdx.x : total;
+            if (L.counter) {
+                const int slot = k & 1;
+                if (!mbar_wait_warp(&uq_full[slot], (k >> 1) & 1, err0, L.wait_ns)) { ok = false; break; }
+                u = uq[slot];
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&uq_empty[slot]);
             }
-            // one 32-column load per wait (two per wait, with the side factors
-            // and sums live, would spill)
-            constexpr int LW = 32;
+            if (u >= total) break;
+            int nb2, i0, i1;
+            int *err;
+            {
+                const T2Unit un = t2_unit<MG>(L, u);
+                nb2 = un.nb2;
+                i0 = un.i0;
+                i1 = un.i1;
+                err = L.g[MG ? un.gi : 0].err;
+            }
+            float S[P], Cc[P];
 #pragma unroll
-            for (int g = 0; g < NG; g++) {
-                if (g >= ngb) break;
-                const int J = (gq + g) * nb2 + j, cs = J & 1;
-                if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, a.err, a.wait_ns)) { ok = false; break; }
-                tc_fence_after();
+            for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
+            float acc[MODE == 0 ? P : 1];  // MODE 0: the item's FP32 sums
 #pragma unroll
-                for (int hh = 0; hh < T2_N / LW; hh++) {
-                    if (g * T2_N + LW * hh >= P * P || g * T2_N + LW * hh >= ncol) break;
-                    uint32_t G[LW];
-                    tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + LW * hh), G);
-                    tmem_wait_ld32(G);
+            for (int p = 0; p < (MODE == 0 ? P : 1); p++) acc[p] = 0.f;
+            for (int it = i0; it < i1; it++) {
+                const int s = q & 1;
+                if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, err, L.wait_ns)) { ok = false; break; }
+                const float *f1s = reinterpret_cast<const float *>(slots + (size_t)(2 * s + j) * region + 2 * T2_ATILE) +
+                                   d * P * VB + v;
+                const int *hoff =
+                    reinterpret_cast<const int *>(slots + (size_t)(2 * s) * region + 2 * T2_ATILE + NDG * P * VB * 4) +
+                    1;
+                const int nch = hoff[P];
+                const bool valid = (nch >> (27 + d)) & 1;
+                const unsigned msk = (unsigned)nch & 0x7ffffffu;
+                const int nl = __popc(msk), ncol = nl * P, ngb = (ncol + T2_N - 1) / T2_N;
+                // Columns n = jj*P + p, jj = the rank of a node of the item's mask.
+                // MODE 0: side = f(c1 + D, l1) of the jj-th node l1 (its offset from
+                //         the slot header; 0 past the mask's nodes),
+                //         acc[p] += side * G[n].
+                // MODE 1: side = c(D, p) (all P live), the sum over p of each jj is
+                //         complete after its P consecutive columns and is kept in
+                //         stg[jj] (local memory: its read index is the rank of a
+                //         node); after the item each node l of the mask adds
+                //         stg[rank(l)] into its (sum, correction).
+                float f1[P], stg[MODE == 1 ? P : 1], run[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                    for (int i = 0; i < LW; i++) {
-                        const int n = g * T2_N + LW * hh + i;
-                        if (n < P * P) {
-                            if constexpr (MODE == 0) {
-                                acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
-                            } else {
-                                // three interleaved partial sums over p
-                                const int pp = n % P, r = pp % 3;
-                                run[r] = pp < 3 ? f1[pp] * __uint_as_float(G[i])
-                                                : fmaf(f1[pp], __uint_as_float(G[i]), run[r]);
-                                if (pp == P - 1) stg[n / P] = (run[0] + run[1]) + run[2];
+                for (int l = 0; l < P; l++) {
+                    if constexpr (MODE == 1) {
+                        f1[l] = f1s[l * VB];
+                    } else {
+                        // loaded before the column loop (the TMEM waits order all
+                        // shared-memory loads, so loads inside it would stall); a
+                        // row the item does not serve gets zero factors, so its
+                        // columns add exact zeros
+                        const int o = hoff[l];
+                        f1[l] = (valid && o >= 0) ? f1s[o] : 0.f;
+                    }
+                }
+                // one 32-column load per wait (two per wait, with the side factors
+                // and sums live, would spill)
+                constexpr int LW = 32;
+#pragma unroll
+                for (int g = 0; g < NG; g++) {
+                    if (g >= ngb) break;
+                    const int J = Jb + g * nb2 + j, cs = J & 1;
+                    if (!mbar_wait_warp(&c_full[cs], (J >> 1) & 1, err, L.wait_ns)) { ok = false; break; }
+                    tc_fence_after();
+#pragma unroll
+                    for (int hh = 0; hh < T2_N / LW; hh++) {
+                        if (g * T2_N + LW * hh >= P * P || g * T2_N + LW * hh >= ncol) break;
+                        uint32_t G[LW];
+                        tmem_ld32_nowait(tl + (uint32_t)(cs * T2_N + LW * hh), G);
+                        tmem_wait_ld32(G);
+#pragma unroll
+                        for (int i = 0; i < LW; i++) {
+                            const int n = g * T2_N + LW * hh + i;
+                            if (n < P * P) {
+                                if constexpr (MODE == 0) {
+                                    acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
+                                } else {
+                                    // three interleaved partial sums over p
+                                    const int pp = n % P, r3 = pp % 3;
+                                    run[r3] = pp < 3 ? f1[pp] * __uint_as_float(G[i])
+                                                     : fmaf(f1[pp], __uint_as_float(G[i]), run[r3]);
+                                    if (pp == P - 1) stg[n / P] = (run[0] + run[1]) + run[2];
+                                }
                             }
                         }
                     }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&c_empty[cs]);
                 }
-                tc_fence_before();
+                if (!ok) break;
+                if constexpr (MODE == 1) {
+                    if (valid) {
+#pragma unroll
+                        for (int p = 0; p < P; p++) {  // two-sum of the node totals into (sum, correction)
+                            if (!((msk >> p) & 1u)) continue;
+                            const float x = stg[__popc(msk & ((1u << p) - 1u))];
+                            const float t = S[p] + x, bpv = t - S[p];
+                            Cc[p] += (S[p] - (t - bpv)) + (x - bpv);
+                            S[p] = t;
+                        }
+                    }
+                }
+                Jb += ngb * nb2;
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&c_empty[cs]);
-            }
-            if (!ok) break;
-            gq += ngb;
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
-            if constexpr (MODE == 0) {
-                // the item's total two-summed into (sum, correction); a row the
-                // item does not serve adds exact zeros (zero side factors)
+                if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
+                if constexpr (MODE == 0) {
+                    // the item's total two-summed into (sum, correction); a row the
+                    // item does not serve adds exact zeros (zero side factors)
 #pragma unroll
-                for (int p = 0; p < P; p++) {
-                    const float t = S[p] + acc[p], bpv = t - S[p];
-                    Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
-                    S[p] = t;
-                    acc[p] = 0.f;
+                    for (int p = 0; p < P; p++) {
+                        const float t = S[p] + acc[p], bpv = t - S[p];
+                        Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
+                        S[p] = t;
+                        acc[p] = 0.f;
+                    }
                 }
-            } else if (valid) {
-#pragma unroll
-                for (int p = 0; p < P; p++) {  // two-sum of the node totals into (sum, correction)
-                    if (!((msk >> p) & 1u)) continue;
-                    const float x = stg[__popc(msk & ((1u << p) - 1u))];
-                    const float t = S[p] + x, bpv = t - S[p];
-                    Cc[p] += (S[p] - (t - bpv)) + (x - bpv);
-                    S[p] = t;
-                }
+                q++;
             }
-            q++;
-        }
-        if (ok) {
-            const int D = D0 + d, vdf = (bt0 + j) * VB + v;
+            if (!ok) continue;
+            // the unit's sums into qacc; persistent launches first wait until the
+            // same rows' previous block set is in
+            const T2Unit un = t2_unit<MG>(L, u);
+            const Tc2Args &a = L.g[MG ? un.gi : 0];
+            int *flag = a.done ? a.done + ((size_t)un.tile * a.nbp + un.bp) * T2_EPI_WARPS + (warp - 2) : nullptr;
+            if (flag) {
+                bool fok = true;
+                if (lane == 0) fok = flag_wait(flag, un.s, a.err, L.wait_ns);
+                if (!__shfl_sync(0xffffffffu, fok ? 1 : 0, 0)) { ok = false; continue; }
+            }
+            const int D = un.tile * NDG + d, vdf = (un.bt0 + j) * VB + v;
             if (D < a.Nc && vdf < a.nvdf) {
                 const double sc = MODE == 0 ? a.inv_scale[vdf] : 1.0;  // the adjoint scales in k_tc_vjp_final
 #pragma unroll
@@ -1249,6 +1415,10 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(Tc2Args a)
                     double *dst = a.qacc + ((size_t)D * P + p) * a.NV + vdf;
                     *dst += ((double)S[p] + (double)Cc[p]) * sc;
                 }
+            }
+            if (flag) {
+                __syncwarp();  // the warp's additions are ordered before lane 0's release
+                if (lane == 0) st_release_gpu(flag, un.s + 1);
             }
         }
     }
@@ -1364,43 +1534,161 @@ static void tc2_sets_adjoint(Ctx *c)
 // the wait limit of the launches, and the one-shot test switch (DGV_OPT_TEST_WITHHOLD:
 // CTA 0 of the first launch arms no copy for its first W stage, so the waits on
 // that stage run out and the call reports DGV_ETIMEOUT)
-static void tc2_wait_args(Ctx *c, Tc2Args &a)
+static void tc2_wait_args(Ctx *c, Tc2Launch &Lh)
 {
-    a.wait_ns = wait_limit_ns(c);
-    a.withhold = c->test_withhold ? 1 : 0;
+    Lh.wait_ns = wait_limit_ns(c);
+    Lh.withhold = c->test_withhold ? 1 : 0;
     c->test_withhold = false;
 }
 
-template <int VB, int P, int MODE = 0>
-static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, const std::vector<int> &sets)
+// a persistent launch needs every unit to hold the same number of VDF tiles:
+// the epilogue warps of a tile that some units lack would run ahead of the
+// tensor-memory accumulators' phases (their parity could then not tell a
+// later phase from a completed one)
+static bool t2_uniform(const Tc2Args &a)
 {
-    const size_t smem = (size_t)T2_NSTW * T2_GREC + 4 * (size_t)a.region + (2 * T2_NSTW + 13) * sizeof(uint64_t) + 16;
-    DGV_CUDA(c, cudaFuncSetAttribute((const void *)k_collide_tc2<VB, P, MODE>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    KTimer kt(c);
-    for (size_t s = 0; s + 1 < sets.size(); s++) {
-        a.item_start = tl.item_start + s * (ng + 1);
-        a.tile_of = tl.tile_of + s * ng;
-        k_collide_tc2<VB, P, MODE><<<(unsigned)(a.nbp * ng), T2_THREADS, smem, c->stream>>>(a);
-        DGV_CUDA(c, cudaGetLastError());
-        a.withhold = 0;  // the test withholds in the first launch only
+    return a.nbt <= a.tpc || a.nbt % a.tpc == 0;
+}
+
+// persistent launches: the order flags (row tile x VDF-tile pair x epilogue
+// warp) and, after them, the unit counter
+static size_t t2_flag_bytes(const Tc2Args &a)
+{
+    return sizeof(int) * ((size_t)a.ng * a.nbp * T2_EPI_WARPS + 1);
+}
+
+// bytes per VDF tile in an item slot: A hi, A lo, the FP32 side tile, the slot header
+static int t2_region(int P, int VB)
+{
+    return (2 * T2_ATILE + (TC_ROWS / VB) * P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
+}
+
+static size_t t2_smem(int region)
+{
+    return (size_t)T2_NSTW * T2_GREC + 4 * (size_t)region + (2 * T2_NSTW + 17) * sizeof(uint64_t) + 16;
+}
+
+// the launch of a block-form kernel: one unit per CTA (grid = units), or
+// persistent (grid = one CTA per SM, launched cooperatively so that all CTAs
+// are resident at once: a CTA may wait for another's flag)
+template <int VB, int P, int MODE, bool MG = false>
+static int t2_launch(Ctx *c, const Tc2Launch &Lh, bool persistent, cudaStream_t stream)
+{
+    const int total = Lh.ubase[Lh.ngrids];
+    if (total <= 0) return DGV_OK;
+    const size_t smem = t2_smem(Lh.region);
+    auto fn = k_collide_tc2<VB, P, MODE, MG>;
+    // the shared-memory limit is raised once per kernel and device (the
+    // attribute call is not free, and every evaluation makes many launches)
+    static int smem_set[64] = {0};
+    if (c->device >= 0 && c->device < 64 && smem_set[c->device] < (int)smem) {
+        DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_set[c->device] = (int)smem;
     }
-    kt.stop((long long)sets.size() - 1);
-    count_launches(c, (long long)sets.size() - 1);
+    if (!persistent) {
+        fn<<<(unsigned)total, T2_THREADS, smem, stream>>>(Lh);
+        DGV_CUDA(c, cudaGetLastError());
+        return DGV_OK;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.blockDim = dim3(T2_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    {
+        int nsm = 148, per_sm = 0;
+        DGV_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+        DGV_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, T2_THREADS, smem));
+        if (per_sm < 1) return set_err(c, DGV_EUNSUP, "block form: the kernel does not fit on an SM");
+        cfg.gridDim = dim3((unsigned)std::min<long long>(total, (long long)nsm * per_sm));
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    DGV_CUDA(c, cudaLaunchKernelEx(&cfg, fn, Lh));
+    return DGV_OK;
+}
+
+// The block form's launches over the block sets of one grid: one launch per
+// set (c->tc_persistent = 0, or a batch whose VDF-tile pairs do not all hold
+// the same number of tiles), or one persistent launch over all sets, whose
+// per-warp order flags (row tile x VDF-tile pair x epilogue warp) start at 0.
+template <int VB, int P, int MODE = 0>
+static int launch_tc2(Ctx *c, Tc2Args &a, const TcLists &tl, const std::vector<int> &sets, int region)
+{
+    Tc2Launch Lh;
+    std::memset(&Lh, 0, sizeof(Lh));
+    Lh.ngrids = 1;
+    Lh.region = region;
+    Lh.tpcmax = std::min(a.tpc, a.nbt);
+    tc2_wait_args(c, Lh);
+    const int nsets = (int)sets.size() - 1, per = a.nbp * a.ng;
+    KTimer kt(c);
+    if (c->tc_persistent && t2_uniform(a)) {
+        const size_t fb = t2_flag_bytes(a);
+        int rc = ensure_buffer(c, &c->d_tc2done, &c->tc2done_bytes, fb);
+        if (rc) return rc;
+        DGV_CUDA(c, cudaMemsetAsync(c->d_tc2done, 0, fb, c->stream));
+        a.item_start = tl.item_start;
+        a.tile_of = tl.tile_of;
+        a.done = reinterpret_cast<int *>(c->d_tc2done);
+        Lh.counter = a.done + (size_t)a.ng * a.nbp * T2_EPI_WARPS;
+        Lh.g[0] = a;
+        Lh.ubase[1] = nsets * per;
+        if ((rc = t2_launch<VB, P, MODE>(c, Lh, true, c->stream))) return rc;
+        kt.stop(1);
+        count_launches(c, 1);
+        return DGV_OK;
+    }
+    a.done = nullptr;
+    Lh.ubase[1] = per;
+    for (int s = 0; s < nsets; s++) {
+        a.item_start = tl.item_start + (size_t)s * (a.ng + 1);
+        a.tile_of = tl.tile_of + (size_t)s * a.ng;
+        Lh.g[0] = a;
+        int rc = t2_launch<VB, P, MODE>(c, Lh, false, c->stream);
+        if (rc) return rc;
+        Lh.withhold = 0;  // the test withholds in the first launch only
+    }
+    kt.stop(nsets);
+    count_launches(c, nsets);
     return DGV_OK;
 }
 
 template <int P, int MODE = 0>
-static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int ng, int VB, const std::vector<int> &sets)
+static int launch_tc2_vb(Ctx *c, Tc2Args &a, const TcLists &tl, int VB, const std::vector<int> &sets, int region)
 {
     switch (VB) {
-    case 128: return launch_tc2<128, P, MODE>(c, a, tl, ng, sets);
-    case 64: return launch_tc2<64, P, MODE>(c, a, tl, ng, sets);
-    default: return launch_tc2<32, P, MODE>(c, a, tl, ng, sets);
+    case 128: return launch_tc2<128, P, MODE>(c, a, tl, sets, region);
+    case 64: return launch_tc2<64, P, MODE>(c, a, tl, sets, region);
+    default: return launch_tc2<32, P, MODE>(c, a, tl, sets, region);
     }
 }
 
-static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
+// the tuned launch choice of this batch class, if the context has one (and the
+// caller set none of the options)
+static void tc2_use_tuned(Ctx *c, int nvdf)
+{
+    if (!c->tc_autotune || c->tc_user_launch) return;
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), nbt = (nvdf + VB - 1) / VB;
+    auto it = c->tc_tuned.find(VB * 2 + (nbt > 1 ? 1 : 0));
+    if (it == c->tc_tuned.end()) return;
+    c->tc_tiles_per_cta = it->second.tiles;
+    c->tc_set_mb = it->second.set_mb;
+    c->tc_persistent = it->second.persistent;
+}
+
+// One block-form evaluation in three parts: tc2_begin (records, sets, work
+// lists, buffers; f in the tile layouts; sums zeroed), the launches, tc2_end
+// (FP64 sums / w, scale, projection).
+struct Tc2Call {
+    Tc2Args a;
+    TcLists tl;
+    int VB = 0, region = 0;
+};
+
+static int tc2_begin(Ctx *c, const double *d_f, int nvdf, Tc2Call &k)
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
@@ -1418,10 +1706,9 @@ static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, do
     if (rc) return rc;
     rc = ensure_buffer(c, &c->d_tcQ, &c->tcQ_bytes, qbytes);
     if (rc) return rc;
-    TcLists tl;
     {
         std::vector<int> first, count;
-        rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl, 1);
+        rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &k.tl, 1);
         if (rc) return rc;
     }
     float *F = reinterpret_cast<float *>(c->d_tcF);
@@ -1432,32 +1719,152 @@ static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, do
     k_tc2_f16<<<1184, 256, 0, c->stream>>>(F, F16, nbt, g.Nc, g.P, VB);
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
-    Tc2Args a;
-    a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.W2 = nullptr; a.items = tl.items;
-    a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
+    count_launches(c, 2);  // k_tc_fprep, k_tc2_f16
+    Tc2Args &a = k.a;
+    std::memset(&a, 0, sizeof(a));
+    a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.W2 = nullptr; a.items = k.tl.items;
+    a.qacc = c->d_tcQ; a.inv_scale = inv; a.err = c->d_err;
     a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
     a.tpc = c->tc_tiles_per_cta;
     a.nbp = (nbt + a.tpc - 1) / a.tpc;
-    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
-    tc2_wait_args(c, a);
-    rc = g.P == 27 ? launch_tc2_vb<27>(c, a, tl, ng, VB, L.tc2_sets) : launch_tc2_vb<8>(c, a, tl, ng, VB, L.tc2_sets);
-    if (rc) return rc;
-    long long tot = (long long)nvdf * g.N;
+    a.ng = ng;
+    k.VB = VB;
+    k.region = t2_region(g.P, VB);
+    // the order flags of persistent launches, allocated here on every call so
+    // that a captured call (graphs of RK steps and of mixed-grid groups) finds
+    // them in place
+    return ensure_buffer(c, &c->d_tc2done, &c->tc2done_bytes, t2_flag_bytes(a));
+}
+
+static int tc2_end(Ctx *c, double *d_q, int nvdf, int NV, double scale)
+{
+    const Grid &g = c->grid;
+    const long long tot = (long long)nvdf * g.N;
     k_tc_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, c->d_nwt, d_q, g.N, nvdf, NV, scale);
     DGV_CUDA(c, cudaGetLastError());
-    count_launches(c, 3);  // k_tc_fprep, k_tc2_f16, k_tc_final
+    count_launches(c, 1);  // k_tc_final
     if (c->project) return project_device(c, d_q, nvdf);
+    return DGV_OK;
+}
+
+static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
+{
+    Tc2Call k;
+    int rc = tc2_begin(c, d_f, nvdf, k);
+    if (rc) return rc;
+    const std::vector<int> &sets = c->lay.tc2_sets;
+    rc = c->grid.P == 27 ? launch_tc2_vb<27>(c, k.a, k.tl, k.VB, sets, k.region)
+                         : launch_tc2_vb<8>(c, k.a, k.tl, k.VB, sets, k.region);
+    if (rc) return rc;
+    return tc2_end(c, d_q, nvdf, k.a.NV, scale);
+}
+
+// Mixed-grid batch (dgv_collide_group) in one persistent launch: members of
+// the block form with the same nodes per cell and VDF tile size (at most
+// T2_MAXG of them).  Each member's preparation runs on its own stream (after
+// `fork` on the origin stream), the launch on the origin stream serves every
+// member's units (grid after grid, each in set order with its own order
+// flags), then each member's final step on its stream; join[i] / join[n + i]
+// bring the members back to the origin.  The members' tuned launch choices
+// (VDF tiles per CTA, records per launch) are kept.
+int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, const int *nb, int n,
+                      cudaStream_t origin, cudaEvent_t fork, cudaEvent_t fork2, const cudaEvent_t *join)
+{
+    Ctx *c0 = cs[0];
+    if (n < 1 || n > T2_MAXG) return set_err(c0, DGV_EUNSUP, "collide_group: persistent launch serves 1-4 grids");
+    const int P = cs[0]->grid.P, VB = nb[0] > 64 ? 128 : (nb[0] > 32 ? 64 : 32);
+    for (int i = 0; i < n; i++) {
+        const int VBi = nb[i] > 64 ? 128 : (nb[i] > 32 ? 64 : 32);
+        if (cs[i]->grid.P != P || (P != 27 && P != 8) || cs[i]->tc_form != 2 || VBi != VB || !cs[i]->lay.tc2_W)
+            return set_err(c0, DGV_EUNSUP, "collide_group: members differ in nodes per cell, form or VDF tile");
+    }
+    for (int i = 0; i < n; i++) tc2_use_tuned(cs[i], nb[i]);
+    Tc2Launch Lh;
+    std::memset(&Lh, 0, sizeof(Lh));
+    Lh.ngrids = n;
+    // every unit of the launch must hold the same number of VDF tiles (checked
+    // before any work is queued)
+    for (int i = 0; i < n; i++) {
+        Tc2Args t;
+        std::memset(&t, 0, sizeof(t));
+        t.nbt = (nb[i] + VB - 1) / VB;
+        t.tpc = cs[i]->tc_tiles_per_cta;
+        const int tpm = std::min(t.tpc, t.nbt);
+        if (!t2_uniform(t) || (i > 0 && tpm != Lh.tpcmax))
+            return set_err(c0, DGV_EUNSUP, "collide_group: the members' units hold different numbers of VDF tiles");
+        Lh.tpcmax = tpm;
+    }
+    tc2_wait_args(c0, Lh);
+    DGV_CUDA(c0, cudaEventRecord(fork, origin));
+    int units = 0;
+    std::vector<int> NVs(n);
+    for (int i = 0; i < n; i++) {
+        Ctx *c = cs[i];
+        if (c->stream != origin) DGV_CUDA(c, cudaStreamWaitEvent(c->stream, fork, 0));
+        Tc2Call k;
+        int rc = tc2_begin(c, f[i], nb[i], k);
+        if (rc) return rc;
+        DGV_CUDA(c, cudaMemsetAsync(c->d_tc2done, 0, t2_flag_bytes(k.a), c->stream));
+        k.a.item_start = k.tl.item_start;
+        k.a.tile_of = k.tl.tile_of;
+        k.a.done = reinterpret_cast<int *>(c->d_tc2done);
+        if (i == 0) Lh.counter = k.a.done + (size_t)k.a.ng * k.a.nbp * T2_EPI_WARPS;  // the launch's unit counter
+        Lh.g[i] = k.a;
+        Lh.region = k.region;
+        Lh.ubase[i] = units;
+        units += ((int)c->lay.tc2_sets.size() - 1) * k.a.nbp * k.a.ng;
+        NVs[i] = k.a.NV;
+        if (c->stream != origin) {
+            DGV_CUDA(c, cudaEventRecord(join[i], c->stream));
+            DGV_CUDA(c0, cudaStreamWaitEvent(origin, join[i], 0));
+        }
+    }
+    Lh.ubase[n] = units;
+    int rc;
+    if (n > 1) {
+        switch (VB) {
+        case 128: rc = P == 27 ? t2_launch<128, 27, 0, true>(c0, Lh, true, origin)
+                               : t2_launch<128, 8, 0, true>(c0, Lh, true, origin); break;
+        case 64: rc = P == 27 ? t2_launch<64, 27, 0, true>(c0, Lh, true, origin)
+                              : t2_launch<64, 8, 0, true>(c0, Lh, true, origin); break;
+        default: rc = P == 27 ? t2_launch<32, 27, 0, true>(c0, Lh, true, origin)
+                              : t2_launch<32, 8, 0, true>(c0, Lh, true, origin); break;
+        }
+    } else {
+        switch (VB) {
+        case 128: rc = P == 27 ? t2_launch<128, 27, 0>(c0, Lh, true, origin)
+                               : t2_launch<128, 8, 0>(c0, Lh, true, origin); break;
+        case 64: rc = P == 27 ? t2_launch<64, 27, 0>(c0, Lh, true, origin)
+                              : t2_launch<64, 8, 0>(c0, Lh, true, origin); break;
+        default: rc = P == 27 ? t2_launch<32, 27, 0>(c0, Lh, true, origin)
+                              : t2_launch<32, 8, 0>(c0, Lh, true, origin); break;
+        }
+    }
+    if (rc) return rc;
+    count_launches(c0, 1);
+    DGV_CUDA(c0, cudaEventRecord(fork2, origin));
+    for (int i = 0; i < n; i++) {
+        Ctx *c = cs[i];
+        if (c->stream != origin) DGV_CUDA(c, cudaStreamWaitEvent(c->stream, fork2, 0));
+        if ((rc = tc2_end(c, q[i], nb[i], NVs[i], 1.0))) return rc;
+        if (c->stream != origin) {
+            DGV_CUDA(c, cudaEventRecord(join[n + i], c->stream));
+            DGV_CUDA(c0, cudaStreamWaitEvent(origin, join[n + i], 0));
+        }
+    }
     return DGV_OK;
 }
 
 // The block form's launch choices, tuned on the first evaluation of each
 // batch class (VDF tile size; one or several VDF tiles): VDF tiles per CTA (two
 // let a block's records cross from L2 once per 256 rows, one gives twice the
-// CTAs) and block records per launch (the records one launch streams should
-// stay in L2 while all its CTAs read them).  Each candidate is evaluated once to
-// warm up (work lists) and once timed with CUDA events on the context stream;
-// the fastest is kept for the context.  Not while the stream is being captured
-// (the current choice serves), and not when the caller set either option.
+// CTAs), block records per launch (the records one launch streams should stay
+// in L2 while all its CTAs read them) and one launch per set or one persistent
+// launch (no tail of short CTAs at the end of each set).  Per records size one
+// evaluation warms up (work lists), then each choice is evaluated once, timed
+// with CUDA events on the context stream; the fastest is kept for the context.
+// Not while the stream is being captured (the current choice serves), and not
+// when the caller set any of the three options.
 static int tc2_autotune(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
 {
     const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32);
@@ -1465,8 +1872,9 @@ static int tc2_autotune(Ctx *c, const double *d_f, double *d_q, int nvdf, double
     const int key = VB * 2 + (nbt > 1 ? 1 : 0);
     auto it = c->tc_tuned.find(key);
     if (it != c->tc_tuned.end()) {
-        c->tc_tiles_per_cta = it->second.first;
-        c->tc_set_mb = it->second.second;
+        c->tc_tiles_per_cta = it->second.tiles;
+        c->tc_set_mb = it->second.set_mb;
+        c->tc_persistent = it->second.persistent;
         return DGV_OK;
     }
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -1481,24 +1889,38 @@ static int tc2_autotune(Ctx *c, const double *d_f, double *d_q, int nvdf, double
     // their records ~10x from DRAM (measured)
     const int tiles[2] = {2, 1}, mbs[2] = {24, 48};
     float best_ms = 1e30f;
-    int best_t = c->tc_tiles_per_cta, best_mb = c->tc_set_mb, rc = DGV_OK;
+    Ctx::TcChoice best{c->tc_tiles_per_cta, c->tc_set_mb, c->tc_persistent};
+    int rc = DGV_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     DGV_CUDA(c, cudaEventCreate(&e0));
     DGV_CUDA(c, cudaEventCreate(&e1));
-    for (int t : tiles) {
-        if (t > 1 && nbt < 2) continue;
-        for (int mb : mbs) {
-            c->tc_tiles_per_cta = t;
-            c->tc_set_mb = mb;
-            if ((rc = collide_tc2_body(c, d_f, d_q, nvdf, scale))) break;
-            cudaEventRecord(e0, c->stream);
-            if ((rc = collide_tc2_body(c, d_f, d_q, nvdf, scale))) break;
-            cudaEventRecord(e1, c->stream);
-            if (cudaEventSynchronize(e1) != cudaSuccess) { rc = set_err(c, DGV_ECUDA, "autotune: event failed"); break; }
-            if ((rc = check_errflag(c))) break;
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best_ms) { best_ms = ms; best_t = t; best_mb = mb; }
+    for (int mb : mbs) {
+        c->tc_set_mb = mb;
+        c->tc_tiles_per_cta = 2;
+        c->tc_persistent = 0;
+        if ((rc = collide_tc2_body(c, d_f, d_q, nvdf, scale))) break;  // warm-up: sets and work lists
+        for (int t : tiles) {
+            if (t > 1 && nbt < 2) continue;
+            const bool uniform = nbt <= t || nbt % t == 0;  // else persistent falls back to per-set launches
+            for (int pe = 0; pe < (uniform ? 2 : 1); pe++) {
+                c->tc_tiles_per_cta = t;
+                c->tc_persistent = pe;
+                cudaEventRecord(e0, c->stream);
+                if ((rc = collide_tc2_body(c, d_f, d_q, nvdf, scale))) break;
+                cudaEventRecord(e1, c->stream);
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    rc = set_err(c, DGV_ECUDA, "autotune: event failed");
+                    break;
+                }
+                if ((rc = check_errflag(c))) break;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = Ctx::TcChoice{t, mb, pe};
+                }
+            }
+            if (rc) break;
         }
         if (rc) break;
     }
@@ -1506,10 +1928,11 @@ static int tc2_autotune(Ctx *c, const double *d_f, double *d_q, int nvdf, double
     cudaEventDestroy(e1);
     c->ktiming = kt;
     c->kt_all = kt_all;
-    c->tc_tiles_per_cta = best_t;
-    c->tc_set_mb = best_mb;
+    c->tc_tiles_per_cta = best.tiles;
+    c->tc_set_mb = best.set_mb;
+    c->tc_persistent = best.persistent;
     if (rc) return rc;
-    c->tc_tuned[key] = {best_t, best_mb};
+    c->tc_tuned[key] = best;
     return DGV_OK;
 }
 
@@ -1617,7 +2040,7 @@ static int tc2_prepare_adjoint(Ctx *c)
     return DGV_OK;
 }
 
-int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int nvdf)
+static int vjp_tc_body(Ctx *c, const double *d_f, const double *d_v, double *d_g, int nvdf)
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
@@ -1659,21 +2082,77 @@ int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, gbytes, c->stream));
     Tc2Args a;
+    std::memset(&a, 0, sizeof(a));
     a.F = Cf; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.W2 = (const unsigned char *)L.tc2_Wv;
-    a.items = tl.items; a.item_start = nullptr; a.tile_of = nullptr; a.qacc = c->d_tcQ; a.inv_scale = nullptr;
+    a.items = tl.items; a.qacc = c->d_tcQ; a.inv_scale = nullptr;
     a.err = c->d_err; a.Nc = g.Nc; a.ccell = g.ccell; a.NV = NV; a.nvdf = nvdf; a.nbt = nbt;
     a.tpc = c->tc_tiles_per_cta;
     a.nbp = (nbt + a.tpc - 1) / a.tpc;
-    a.region = (2 * T2_ATILE + NDG * g.P * VB * 4 + T2_HDR + 1023) / 1024 * 1024;
-    tc2_wait_args(c, a);
-    rc = g.P == 27 ? launch_tc2_vb<27, 1>(c, a, tl, ng, VB, L.tc2_sets_adj)
-                   : launch_tc2_vb<8, 1>(c, a, tl, ng, VB, L.tc2_sets_adj);
+    a.ng = ng;
+    const int region = t2_region(g.P, VB);
+    rc = g.P == 27 ? launch_tc2_vb<27, 1>(c, a, tl, VB, L.tc2_sets_adj, region)
+                   : launch_tc2_vb<8, 1>(c, a, tl, VB, L.tc2_sets_adj, region);
     if (rc) return rc;
     const long long tot = (long long)nvdf * g.N;
     k_tc_vjp_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, inv_f, inv_c, d_g, g.N, nvdf, NV);
     DGV_CUDA(c, cudaGetLastError());
     count_launches(c, 4);  // k_tc_fprep, k_tc2_f16, k_tc_cprep, k_tc_vjp_final
     return DGV_OK;
+}
+
+// The adjoint uses the collision operator's tuned VDF tiles per CTA and
+// records per launch (its sets hold that many MB of W and W2 records
+// together); one launch per set or one persistent launch is chosen on its
+// own first call per batch class (evaluated once each after a warm-up, CUDA
+// events on the context stream), unless the caller set DGV_OPT_TCPERSIST.
+int vjp_tc_device(Ctx *c, const double *d_f, const double *d_v, double *d_g, int nvdf)
+{
+    tc2_use_tuned(c, nvdf);
+    if (!c->tc_autotune || c->tc_user_launch) return vjp_tc_body(c, d_f, d_v, d_g, nvdf);
+    const int VB = nvdf > 64 ? 128 : (nvdf > 32 ? 64 : 32), nbt = (nvdf + VB - 1) / VB;
+    const int key = VB * 2 + (nbt > 1 ? 1 : 0);
+    const int saved = c->tc_persistent;
+    int pers = 0, rc = DGV_OK;
+    auto it = c->tc_tuned_adj.find(key);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    DGV_CUDA(c, cudaStreamIsCapturing(c->stream, &cap));
+    if (it != c->tc_tuned_adj.end()) {
+        pers = it->second;
+    } else if (cap == cudaStreamCaptureStatusNone) {
+        const bool kt = c->ktiming;
+        const long long kt_all = c->kt_all;
+        c->ktiming = false;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        DGV_CUDA(c, cudaEventCreate(&e0));
+        DGV_CUDA(c, cudaEventCreate(&e1));
+        float best = 1e30f;
+        c->tc_persistent = 0;
+        rc = vjp_tc_body(c, d_f, d_v, d_g, nvdf);  // warm-up: adjoint records, sets, work lists
+        for (int pe = 0; pe < 2 && !rc; pe++) {
+            c->tc_persistent = pe;
+            cudaEventRecord(e0, c->stream);
+            if ((rc = vjp_tc_body(c, d_f, d_v, d_g, nvdf))) break;
+            cudaEventRecord(e1, c->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                rc = set_err(c, DGV_ECUDA, "autotune: event failed");
+                break;
+            }
+            if ((rc = check_errflag(c))) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; pers = pe; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c->ktiming = kt;
+        c->kt_all = kt_all;
+        if (rc) { c->tc_persistent = saved; return rc; }
+        c->tc_tuned_adj[key] = pers;
+    }
+    c->tc_persistent = pers;
+    rc = vjp_tc_body(c, d_f, d_v, d_g, nvdf);
+    c->tc_persistent = saved;
+    return rc;
 }
 
 template <int VB>
@@ -1719,8 +2198,9 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
         if (c->tc_autotune && !c->tc_user_launch) {  // the choice tuned for this batch class, if any
             auto it = c->tc_tuned.find(VB * 2 + (nbt > 1 ? 1 : 0));
             if (it != c->tc_tuned.end()) {
-                c->tc_tiles_per_cta = it->second.first;
-                c->tc_set_mb = it->second.second;
+                c->tc_tiles_per_cta = it->second.tiles;
+                c->tc_set_mb = it->second.set_mb;
+                c->tc_persistent = it->second.persistent;
             }
         }
         tc2_sets(c);
@@ -1728,7 +2208,9 @@ int tc_plan(Ctx *c, int nvdf, long long *launches, long long *items, double *flo
         if ((rc = tc_work_lists(c, NDG, 256 + NDG, L.tc2_sets, first, count, &tl, 1))) return rc;
         // per item and VDF tile: 2 K steps x 3 split products over its issued columns
         const long long cols = L.tc_list_work[256 + NDG];
-        *launches = (long long)L.tc2_sets.size() - 1;
+        const int tpc = c->tc_tiles_per_cta;
+        const bool uniform = nbt <= tpc || nbt % tpc == 0;
+        *launches = c->tc_persistent && uniform ? 1 : (long long)L.tc2_sets.size() - 1;
         *items = L.tc_list_items[256 + NDG] * nbt;
         *flop = (double)cols * nbt * 6.0 * 2.0 * TC_ROWS * 16;
     } else {

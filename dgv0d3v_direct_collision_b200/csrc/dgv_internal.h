@@ -149,8 +149,15 @@ struct Ctx {
     long long wait_limit_us = 0;  // DGV_OPT_WAIT_LIMIT_US: bounded waits of the block form (0 = 4 s)
     int f_global = 0;             // DGV_OPT_FGLOBAL: 1 = CUDA-core kernels gather f from global memory
     bool tc_autotune = true;      // DGV_OPT_TCAUTOTUNE: tune tiles per CTA and records per launch
-    bool tc_user_launch = false;  // the caller set DGV_OPT_TCTILES or DGV_OPT_TCSETMB: no tuning
-    std::map<int, std::pair<int, int>> tc_tuned;  // per batch class: (tiles per CTA, MB per launch)
+    int tc_persistent = 0;     // DGV_OPT_TCPERSIST: block form, 1 = one persistent launch over all block sets
+    bool tc_user_launch = false;  // the caller set DGV_OPT_TCTILES, _TCSETMB or _TCPERSIST: no tuning
+    struct TcChoice {
+        int tiles, set_mb, persistent;
+    };
+    std::map<int, TcChoice> tc_tuned;  // per batch class: the tuned launch choice
+    std::map<int, int> tc_tuned_adj;   // per batch class: the adjoint's persistent-launch choice
+    double *d_tc2done = nullptr;       // persistent block-form launches: order flags (ints)
+    size_t tc2done_bytes = 0;
     bool test_withhold = false;   // DGV_OPT_TEST_WITHHOLD: the next block-form launch withholds one copy
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending, kt_pool;
     long long kt_launches = 0, kt_all = 0;

@@ -8,6 +8,9 @@
 // eagerly (it settles autotuned chunk counts, work lists and buffers); the
 // second captures the whole fork/join into one CUDA graph; later calls replay
 // it with a single launch.  The members' kernels may overlap on the device.
+// On the tensor cores (block form, same nodes per cell and VDF tile size, at
+// most four members) the captured graph holds one persistent collision kernel
+// for all members instead of one launch per member and block set.
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -18,6 +21,8 @@
 namespace dgv {
 
 int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, double scale);
+int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, const int *nb, int n,
+                      cudaStream_t origin, cudaEvent_t fork, cudaEvent_t fork2, const cudaEvent_t *join);
 
 namespace {
 
@@ -51,10 +56,33 @@ struct GroupGraph {
 std::map<GroupKey, GroupGraph> g_groups;
 std::recursive_mutex g_groups_mu;
 
-// fork from origin to every member stream, run the members, join back
-int run_members(const GroupKey &k, cudaEvent_t fork, std::vector<cudaEvent_t> &join)
+// fork from origin to every member stream, run the members, join back; with
+// `persistent`, members on the tensor cores' block form that can share one
+// launch are served by one persistent kernel (collide_tc2_group)
+int run_members(const GroupKey &k, cudaEvent_t fork, cudaEvent_t fork2, std::vector<cudaEvent_t> &join,
+                bool persistent)
 {
     Ctx *c0 = k.m[0].c;
+    if (persistent && k.precision == DGV_PREC_TC && k.m.size() <= 4) {
+        std::vector<Ctx *> cs;
+        std::vector<const double *> fs;
+        std::vector<double *> qs;
+        std::vector<int> nbs;
+        bool proj_ok = true;
+        for (const Member &mb : k.m) {
+            cs.push_back(mb.c);
+            fs.push_back(mb.f);
+            qs.push_back(mb.q);
+            nbs.push_back(mb.nb);
+            proj_ok = proj_ok && (mb.project != 0) == mb.c->project;
+        }
+        if (proj_ok) {
+            const int rc = collide_tc2_group(cs.data(), fs.data(), qs.data(), nbs.data(), (int)cs.size(), k.origin,
+                                             fork, fork2, join.data());
+            if (rc != DGV_EUNSUP) return rc;
+            c0->err.clear();  // members that cannot share a launch: one call per member
+        }
+    }
     DGV_CUDA(c0, cudaEventRecord(fork, k.origin));
     for (size_t i = 0; i < k.m.size(); i++) {
         const Member &mb = k.m[i];
@@ -71,11 +99,12 @@ int run_members(const GroupKey &k, cudaEvent_t fork, std::vector<cudaEvent_t> &j
 }
 
 struct Events {
-    cudaEvent_t fork = nullptr;
+    cudaEvent_t fork = nullptr, fork2 = nullptr;
     std::vector<cudaEvent_t> join;
     ~Events()
     {
         if (fork) cudaEventDestroy(fork);
+        if (fork2) cudaEventDestroy(fork2);
         for (cudaEvent_t e : join)
             if (e) cudaEventDestroy(e);
     }
@@ -130,7 +159,8 @@ extern "C" int dgv_collide_group(int32_t n, dgv_ctx *const *ctxs, const int32_t 
     DGV_CUDA(c0, cudaSetDevice(c0->device));
     Events ev;
     DGV_CUDA(c0, cudaEventCreateWithFlags(&ev.fork, cudaEventDisableTiming));
-    ev.join.assign(key.m.size(), nullptr);
+    DGV_CUDA(c0, cudaEventCreateWithFlags(&ev.fork2, cudaEventDisableTiming));
+    ev.join.assign(2 * key.m.size(), nullptr);
     for (auto &e : ev.join) DGV_CUDA(c0, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 
     // propagate a member's error message to the first context
@@ -148,14 +178,14 @@ extern "C" int dgv_collide_group(int32_t n, dgv_ctx *const *ctxs, const int32_t 
             DGV_CUDA(c0, cudaGraphLaunch(gr.exec, key.origin));
             for (size_t i = 0; i < key.m.size(); i++) count_launches(key.m[i].c, gr.launches[i]);
         } else if (gr.calls++ == 0) {
-            int rc = run_members(key, ev.fork, ev.join);
+            int rc = run_members(key, ev.fork, ev.fork2, ev.join, false);
             if (rc) return fail(rc);
         } else {
             std::vector<long long> before;
             for (const Member &mb : key.m) before.push_back(mb.c->kt_all);
             cudaGraph_t graph = nullptr;
             DGV_CUDA(c0, cudaStreamBeginCapture(key.origin, cudaStreamCaptureModeThreadLocal));
-            int rc = run_members(key, ev.fork, ev.join);
+            int rc = run_members(key, ev.fork, ev.fork2, ev.join, true);
             cudaError_t e = cudaStreamEndCapture(key.origin, &graph);
             if (rc) {
                 if (graph) cudaGraphDestroy(graph);

@@ -165,6 +165,13 @@ class DGVSolver:
         """Block form: megabytes of block records per kernel launch."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCSETMB, int(mb)))
 
+    def set_tc_persistent(self, on: bool):
+        """Block form: one persistent launch over all block sets (1) or one
+        launch per set (0) -- the same results bit for bit
+        (DGV_OPT_TCPERSIST; setting it switches the launch tuning off)."""
+        from ._lib import DGV_OPT_TCPERSIST
+        self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCPERSIST, int(on)))
+
     def set_f_global(self, on: bool):
         """CUDA-core kernels gather f from a local-major copy in global memory
         instead of staging it in shared memory (DGV_OPT_FGLOBAL; grids whose f

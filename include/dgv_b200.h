@@ -72,10 +72,16 @@ extern "C" {
                                  /* DGV_ETIMEOUT                              */
 #define DGV_OPT_TCAUTOTUNE 9      /* block form: 1 (default) = on the first    */
                                  /* evaluation of each batch class, time VDF  */
-                                 /* tiles per CTA x records per launch and    */
-                                 /* keep the fastest; 0 = the options' values */
-                                 /* (setting DGV_OPT_TCTILES or _TCSETMB also */
-                                 /* switches the tuning off)                  */
+                                 /* tiles per CTA x records per launch x      */
+                                 /* persistent or not, keep the fastest; 0 =  */
+                                 /* the options' values (setting _TCTILES,    */
+                                 /* _TCSETMB or _TCPERSIST also switches the  */
+                                 /* tuning off)                               */
+#define DGV_OPT_TCPERSIST 11     /* block form: 1 = one persistent launch (one */
+                                 /* CTA per SM) over all sets of records,     */
+                                 /* each set's sums added in set order; 0 =   */
+                                 /* one launch per set (same results, bit for */
+                                 /* bit)                                      */
 #define DGV_OPT_FGLOBAL 10        /* CUDA-core kernels (FP64, FP32-compensated, */
                                  /* mixed terms, FP64 adjoint): 0 (default) = */
                                  /* f of a VDF staged in shared memory when   */

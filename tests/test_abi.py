@@ -78,6 +78,7 @@ def test_status_codes_match_header():
     for name in ("DGV_OK", "DGV_EINVAL", "DGV_ERANGE", "DGV_ECUDA", "DGV_ETIMEOUT", "DGV_ENOMEM",
                  "DGV_ESTATE", "DGV_EUNSUP", "DGV_PREC_F64", "DGV_PREC_F32C", "DGV_PREC_TC", "DGV_OPT_PROJECT",
                  "DGV_OPT_NCHUNKS", "DGV_OPT_KTIMING", "DGV_OPT_TCFORM", "DGV_OPT_TCTILES", "DGV_OPT_TCSETMB",
-                 "DGV_OPT_WAIT_LIMIT_US", "DGV_OPT_TEST_WITHHOLD", "DGV_OPT_TCAUTOTUNE", "DGV_OPT_FGLOBAL"):
+                 "DGV_OPT_WAIT_LIMIT_US", "DGV_OPT_TEST_WITHHOLD", "DGV_OPT_TCAUTOTUNE", "DGV_OPT_FGLOBAL",
+                 "DGV_OPT_TCPERSIST"):
         val = int(re.search(r"#define\s+%s\s+(\d+)" % name, src).group(1))
         assert getattr(_lib, name) == val, name

@@ -129,6 +129,7 @@ def test_tc2_launch_size_option(c1):
     number of launches, not the result."""
     o, s = c1["oracle"], c1["solver"]
     fs = np.stack([o.maxwellian(1.0, 0.2 * k, 0, 0, 0.7) for k in range(20)])
+    s.set_tc_persistent(False)  # one launch per set of records
     q48 = s.EvalCollisionPeriodicAPlus_DGV(fs, precision="tc")
     n48 = s.tc_plan(20)["launches"]
     s.set_tc_set_mb(8)
