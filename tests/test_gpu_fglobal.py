@@ -33,6 +33,9 @@ def test_fglobal_forced_equals_shared(grid):
     s = m.DGVSolver(*grid)
     try:
         s.generate_synthetic_A(seed=11, support=1)
+        # a fixed number of block chunks: small batches otherwise time their
+        # chunk count, and a different partition sums in a different order
+        s.set_nchunks(64)
         f, d = _pair(s)
         rng = np.random.default_rng(9)
         v = rng.standard_normal(s.N)
