@@ -15,6 +15,7 @@ DGV_OK, DGV_EINVAL, DGV_ERANGE, DGV_ECUDA, DGV_ETIMEOUT, DGV_ENOMEM, DGV_ESTATE,
 DGV_PREC_F64, DGV_PREC_F32C, DGV_PREC_TC = 0, 1, 2
 DGV_OPT_PROJECT, DGV_OPT_NCHUNKS, DGV_OPT_KTIMING, DGV_OPT_TCFORM, DGV_OPT_TCTILES, DGV_OPT_TCSETMB = 1, 2, 3, 4, 5, 6
 DGV_OPT_WAIT_LIMIT_US, DGV_OPT_TEST_WITHHOLD, DGV_OPT_TCAUTOTUNE, DGV_OPT_FGLOBAL, DGV_OPT_TCPERSIST = 7, 8, 9, 10, 11
+DGV_LAYOUT_F32, DGV_LAYOUT_TC_CHUNK, DGV_LAYOUT_TC_BLOCK, DGV_LAYOUT_TC_ADJ = 1, 2, 4, 8
 
 STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4: "DGV_ETIMEOUT",
                 5: "DGV_ENOMEM", 6: "DGV_ESTATE", 7: "DGV_EUNSUP"}
@@ -22,7 +23,7 @@ STATUS_NAMES = {0: "DGV_OK", 1: "DGV_EINVAL", 2: "DGV_ERANGE", 3: "DGV_ECUDA", 4
 # every entry point include/dgv_b200.h declares
 EXPORTS = [
     "dgv_ctx_create", "dgv_ctx_destroy", "dgv_last_error", "dgv_set_stream", "dgv_set_async",
-    "dgv_set_option", "dgv_get_option", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
+    "dgv_set_option", "dgv_get_option", "dgv_release_layouts", "dgv_kernel_stats", "dgv_grid_info", "dgv_nodes", "dgv_load_A", "dgv_generate_A_synthetic",
     "dgv_A_info", "dgv_export_A", "dgv_collide", "dgv_collide_batched", "dgv_collide_cells", "dgv_spatial_oper", "dgv_set_regime",
     "dgv_regime_info",
     "dgv_step_rk", "dgv_step_rk_batched", "dgv_prepare_ab", "dgv_step_ab", "dgv_moments", "dgv_maxwellian", "dgv_project",
@@ -102,6 +103,7 @@ def load() -> C.CDLL:
         "dgv_vjp": [vp, vp, vp, vp, C.c_int],
         "dgv_vjp_batched": [vp, i32, vp, vp, vp, C.c_int],
         "dgv_get_option": [vp, C.c_int, C.POINTER(C.c_int64)],
+        "dgv_release_layouts": [vp, C.c_int, C.POINTER(C.c_int64)],
         "dgv_prepare_linear": [vp, vp],
         "dgv_apply_linear": [vp, vp, vp, C.c_int],
         "dgv_collide_f64_noalloc": [vp, vp, vp, i32, vp],

@@ -406,6 +406,21 @@ int dgv_get_option(dgv_ctx *ctx, int option, int64_t *value)
     }
 }
 
+int dgv_release_layouts(dgv_ctx *ctx, int mask, int64_t *freed_bytes)
+{
+    CTX_CHECK(ctx);
+    Ctx *c = &ctx->c;
+    if (mask & ~(DGV_LAYOUT_F32 | DGV_LAYOUT_TC_CHUNK | DGV_LAYOUT_TC_BLOCK | DGV_LAYOUT_TC_ADJ))
+        return set_err(c, DGV_EINVAL, "release_layouts: unknown layout bits");
+    size_t free0 = 0, free1 = 0, total = 0;
+    DGV_CUDA(c, cudaMemGetInfo(&free0, &total));
+    int rc = release_layouts(c, mask);
+    if (rc) return rc;
+    DGV_CUDA(c, cudaMemGetInfo(&free1, &total));
+    if (freed_bytes) *freed_bytes = (int64_t)free1 - (int64_t)free0;
+    return DGV_OK;
+}
+
 int dgv_kernel_stats(dgv_ctx *ctx, double *ms, int64_t *launches, int64_t *all_launches, int reset)
 {
     CTX_CHECK(ctx);

@@ -329,6 +329,48 @@ __global__ void k_f_local_major(const double *f, T *out, long long N, int Nc, in
 // basis functions per CTA of the sliced kernels, and the slices of a grid
 static int p_slices(int P) { return P > 27 ? (P + P_SLICE - 1) / P_SLICE : 1; }
 
+// FP32 rows from the FP64 rows: offsets copied, values rounded to nearest
+// (as the layout builders write them)
+__global__ void k_rows32_from64(const double *rows64, int RD64, float *rows32, int RW32, int P,
+                                       long long npairs)
+{
+    const long long tot = npairs * RW32;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+        const long long k = i / RW32;
+        const int w = (int)(i - k * RW32);
+        const double *r = rows64 + (size_t)k * RD64;
+        float x = 0.f;
+        if (w < 2) {
+            int o[2];
+            memcpy(o, r, 8);
+            x = __int_as_float(o[w]);
+        } else if (w - 2 < P) {
+            x = __double2float_rn(r[1 + (w - 2)]);
+        }
+        rows32[i] = x;
+    }
+}
+
+int ensure_rows32(Ctx *c)
+{
+    Layout &L = c->lay;
+    if (L.rows32 || !L.rows64) return DGV_OK;
+    const size_t bytes = (size_t)std::max<long long>(1, L.npairs) * L.RW32 * sizeof(float);
+    cudaError_t e = cudaMalloc(&L.rows32, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        L.rows32 = nullptr;
+        return set_err(c, DGV_ENOMEM, "FP32 rows: no room on the device");
+    }
+    if (L.npairs) {
+        k_rows32_from64<<<148 * 8, 256, 0, c->stream>>>((const double *)L.rows64, L.RD64, (float *)L.rows32, L.RW32,
+                                                      c->grid.P, L.npairs);
+        DGV_CUDA(c, cudaGetLastError());
+        count_launches(c, 1);
+    }
+    return DGV_OK;
+}
+
 int f_local_major(Ctx *c, const double *d_f, int nvdf, bool f32, const void **out)
 {
     const Grid &g = c->grid;
@@ -398,6 +440,7 @@ static int run_collide(Ctx *c, const double *d_f, const double *d_f2, double *d_
     LaunchShape sh;
     int rc = shape_for(c, mode, sh, cell1 - cell0);
     if (rc) return rc;
+    if (mode == MODE_F32C && (rc = ensure_rows32(c))) return rc;  // rebuilt if released
     KernelFn fn = pick_kernel(g.P, mode, sh.gf);
     if (!fn) return set_err(c, DGV_EUNSUP, "collide: this build supports 1, 8, 27 or 125 nodes per cell");
     DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));

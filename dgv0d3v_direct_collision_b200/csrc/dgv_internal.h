@@ -187,6 +187,10 @@ int set_err(Ctx *c, int code, const std::string &msg);
     } while (0)
 
 int ensure_buffer(Ctx *c, double **p, size_t *have, size_t need_bytes);
+// frees the layouts of a DGV_LAYOUT_* mask (rebuilt on their next use)
+int release_layouts(Ctx *c, int mask);
+// the FP32 rows, rebuilt from the FP64 rows after a release
+int ensure_rows32(Ctx *c);
 // local-major copies f[v][l*Nc + cell] of nvdf VDFs (FP32 or FP64) in the
 // context's buffer, for the CUDA-core kernels that gather f from global memory
 int f_local_major(Ctx *c, const double *d_f, int nvdf, bool f32, const void **out);

@@ -35,6 +35,59 @@ void free_layout(Layout &L)
     L = Layout();
 }
 
+// Frees the device layouts of `mask` (DGV_LAYOUT_*); each is rebuilt on its
+// next use (FP32 rows from the FP64 rows by ensure_rows32, the tensor-core
+// records by their prepare functions).  Graphs holding launches that read
+// them are released first.
+int release_layouts(Ctx *c, int mask)
+{
+    Layout &L = c->lay;
+    release_graphs(c);
+    DGV_CUDA(c, cudaStreamSynchronize(c->stream));
+    auto drop_lists = [&](int lo, int hi) {  // work lists keyed in [lo, hi)
+        for (auto it = L.tc_lists.begin(); it != L.tc_lists.end();) {
+            if (it->first >= lo && it->first < hi) {
+                for (void *q : it->second) cudaFree(q);
+                L.tc_list_work.erase(it->first);
+                L.tc_list_items.erase(it->first);
+                it = L.tc_lists.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    };
+    if ((mask & DGV_LAYOUT_F32) && L.rows32) {
+        cudaFree(L.rows32);
+        L.rows32 = nullptr;
+    }
+    if (mask & DGV_LAYOUT_TC_CHUNK) {
+        if (L.tc_V) cudaFree(L.tc_V);
+        if (L.tc_chunk_start) cudaFree(L.tc_chunk_start);
+        L.tc_V = nullptr;
+        L.tc_chunk_start = nullptr;
+        L.tc_chunk_host.clear();
+        L.tc_sets.clear();
+        drop_lists(0, 256);
+    }
+    if (mask & (DGV_LAYOUT_TC_BLOCK | DGV_LAYOUT_TC_ADJ)) {
+        if (L.tc2_Wv) cudaFree(L.tc2_Wv);
+        L.tc2_Wv = nullptr;
+        L.tc2_goff2.clear();
+        L.tc2_sets_adj.clear();
+        drop_lists(512, 1 << 30);
+    }
+    if (mask & DGV_LAYOUT_TC_BLOCK) {
+        if (L.tc2_W) cudaFree(L.tc2_W);
+        L.tc2_W = nullptr;
+        L.tc2_mask.clear();
+        L.tc2_goff.clear();
+        L.tc2_sets.clear();
+        L.tc2_set_mb = 0;
+        drop_lists(256, 512);
+    }
+    return DGV_OK;
+}
+
 static inline void box_for(const Grid &g, int c1, int c2, BlockInfo &b)
 {
     int a[3] = {g.cell_u(c1), g.cell_v(c1), g.cell_w(c1)};

@@ -165,6 +165,19 @@ class DGVSolver:
         """Block form: megabytes of block records per kernel launch."""
         self._check(self._lib.dgv_set_option(self._h, DGV_OPT_TCSETMB, int(mb)))
 
+    def release_layouts(self, f32: bool = False, tc_chunk: bool = False, tc_block: bool = False,
+                        tc_adjoint: bool = False) -> int:
+        """Frees device layouts that are not needed (dgv_release_layouts):
+        the FP32 rows, the chunk-form or block-form tensor-core records, or
+        only the block-form adjoint's second record set.  Each is rebuilt on
+        its next use.  Returns the change in the device's free memory."""
+        from ._lib import DGV_LAYOUT_F32, DGV_LAYOUT_TC_ADJ, DGV_LAYOUT_TC_BLOCK, DGV_LAYOUT_TC_CHUNK
+        mask = ((DGV_LAYOUT_F32 if f32 else 0) | (DGV_LAYOUT_TC_CHUNK if tc_chunk else 0) |
+                (DGV_LAYOUT_TC_BLOCK if tc_block else 0) | (DGV_LAYOUT_TC_ADJ if tc_adjoint else 0))
+        freed = C.c_int64()
+        self._check(self._lib.dgv_release_layouts(self._h, mask, C.byref(freed)))
+        return freed.value
+
     def set_tc_persistent(self, on: bool):
         """Block form: one persistent launch over all block sets (1) or one
         launch per set (0) -- the same results bit for bit

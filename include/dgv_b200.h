@@ -93,6 +93,12 @@ extern "C" {
                                  /* unissued, so its waits run out and it     */
                                  /* returns DGV_ETIMEOUT; resets itself       */
 
+/* layouts for dgv_release_layouts */
+#define DGV_LAYOUT_F32 1      /* FP32 rows of the pair layout (FP32-compensated Q) */
+#define DGV_LAYOUT_TC_CHUNK 2 /* records of the tensor-core chunk form          */
+#define DGV_LAYOUT_TC_BLOCK 4 /* records of the block form and of its adjoint   */
+#define DGV_LAYOUT_TC_ADJ 8   /* only the adjoint's second record set           */
+
 typedef struct dgv_ctx dgv_ctx;
 
 /* Uniform velocity grid (SetDGVblzmmesh + Set3DCellsR_DGVblzm + SetNodesDGV,
@@ -122,6 +128,14 @@ int dgv_set_option(dgv_ctx *ctx, int option, int64_t value);
  * of an option (for DGV_OPT_TCTILES / DGV_OPT_TCSETMB: the choice the
  * autotuner made for the last batch class evaluated) */
 int dgv_get_option(dgv_ctx *ctx, int option, int64_t *value);
+/* Frees device layouts the caller does not need (DGV_LAYOUT_* mask): the FP32
+ * rows (7 GB at 27^3, built when A is loaded), the records of either
+ * tensor-core form (built on first use: 8 GB chunk, 12 GB block, 12 GB more for
+ * the block form's adjoint at 27^3).  Each is rebuilt on its next use, with the
+ * same values (FP32 rows from the FP64 rows, records from the pair layout);
+ * CUDA graphs of the context are released.  *freed_bytes (may be NULL) gets
+ * the change in the device's free memory.  No counterpart in the reference. */
+int dgv_release_layouts(dgv_ctx *ctx, int mask, int64_t *freed_bytes);
 /* No counterpart in the reference (measurement hook): summed device time in
  * ms and launch count of the collision kernel (k_collide_tc / k_collide_pipe)
  * over the calls made since the last reset while DGV_OPT_KTIMING was on,

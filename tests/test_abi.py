@@ -79,6 +79,7 @@ def test_status_codes_match_header():
                  "DGV_ESTATE", "DGV_EUNSUP", "DGV_PREC_F64", "DGV_PREC_F32C", "DGV_PREC_TC", "DGV_OPT_PROJECT",
                  "DGV_OPT_NCHUNKS", "DGV_OPT_KTIMING", "DGV_OPT_TCFORM", "DGV_OPT_TCTILES", "DGV_OPT_TCSETMB",
                  "DGV_OPT_WAIT_LIMIT_US", "DGV_OPT_TEST_WITHHOLD", "DGV_OPT_TCAUTOTUNE", "DGV_OPT_FGLOBAL",
-                 "DGV_OPT_TCPERSIST"):
+                 "DGV_OPT_TCPERSIST", "DGV_LAYOUT_F32", "DGV_LAYOUT_TC_CHUNK", "DGV_LAYOUT_TC_BLOCK",
+                 "DGV_LAYOUT_TC_ADJ"):
         val = int(re.search(r"#define\s+%s\s+(\d+)" % name, src).group(1))
         assert getattr(_lib, name) == val, name
