@@ -1584,13 +1584,7 @@ static int t2_launch(Ctx *c, const Tc2Launch &Lh, bool persistent, cudaStream_t 
     if (total <= 0) return DGV_OK;
     const size_t smem = t2_smem(Lh.region);
     auto fn = k_collide_tc2<VB, P, MODE, MG>;
-    // the shared-memory limit is raised once per kernel and device (the
-    // attribute call is not free, and every evaluation makes many launches)
-    static int smem_set[64] = {0};
-    if (c->device >= 0 && c->device < 64 && smem_set[c->device] < (int)smem) {
-        DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        smem_set[c->device] = (int)smem;
-    }
+    DGV_CUDA(c, cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (!persistent) {
         fn<<<(unsigned)total, T2_THREADS, smem, stream>>>(Lh);
         DGV_CUDA(c, cudaGetLastError());
