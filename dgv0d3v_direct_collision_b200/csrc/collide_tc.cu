@@ -894,23 +894,101 @@ __global__ void k_tc2_build(const BlockInfo *blk, const double *rows64, int RD64
 // F16[((bt*2 + h)*Nc + cell) * VB*64 + t2_off(v, l)]: per VDF tile and cell a
 // tile of VB rows (VDFs) x 32 nodes, h = 0 hi / 1 lo parts of the scaled FP32
 // copy F[((bt*Nc + cell)*P + l)*VB + v]; nodes l >= P are zero
-__global__ void k_tc2_f16(const float *F, unsigned char *F16, int nbt, int Nc, int P, int VB)
+constexpr int T2_MAXG = 4;  // grids of one launch (mixed-grid batches)
+
+// Per call, for the grids of one launch (one, or the members of a mixed-grid
+// group): per VDF slot v (one CTA; slots past nvdf are zero rows) the
+// power-of-two scale of f (max |f| -> [32, 64)), the scaled FP32 side tile
+// F[bt][cell][l][lb] and its split fp16 operand tiles (hi, lo) in the MMA's
+// A layout, nodes l >= P zero; inv_scale[v] undoes the scale in the result
+// (f enters it pw times).
+struct Tc2PrepGrid {
+    const double *f;
+    float *F;
+    unsigned char *F16;
+    double *inv_scale;
+    long long N;
+    int nvdf, NV, Nc, P, VB, pw;
+    double vinv;
+};
+struct Tc2PrepLaunch {
+    Tc2PrepGrid g[T2_MAXG];
+    int ngrids;
+    int vbase[T2_MAXG + 1];  // first CTA of each grid
+};
+
+__global__ void k_tc2_prep(const __grid_constant__ Tc2PrepLaunch A)
 {
-    const long long total = (long long)nbt * Nc * T2_K * VB;
-    const size_t tile = (size_t)VB * T2_K * 2;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int v = (int)(i % VB);
-        long long r = i / VB;
-        const int l = (int)(r % T2_K);
-        r /= T2_K;
-        const int cell = (int)(r % Nc), bt = (int)(r / Nc);
-        const float x = l < P ? F[(((size_t)bt * Nc + cell) * P + l) * VB + v] : 0.f;
+    int gi = 0;
+    while (gi + 1 < A.ngrids && (int)blockIdx.x >= A.vbase[gi + 1]) gi++;
+    const Tc2PrepGrid &G = A.g[gi];
+    const int v = blockIdx.x - A.vbase[gi];
+    __shared__ double red[32];
+    double m = 0.0;
+    if (v < G.nvdf)
+        for (long long i = threadIdx.x; i < G.N; i += blockDim.x) m = fmax(m, fabs(G.f[(size_t)v * G.N + i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) red[0] = m;
+    }
+    __syncthreads();
+    m = red[0];
+    int e = 0;
+    if (m > 0.0) {
+        frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
+        e = 6 - e;
+    }
+    const double sc = ldexp(1.0, e);
+    if (threadIdx.x == 0) G.inv_scale[v] = ldexp(1.0, -G.pw * e) * G.vinv;
+    const int bt = v / G.VB, lb = v % G.VB, P = G.P;
+    const size_t tile = (size_t)G.VB * T2_K * 2;
+    for (long long i = threadIdx.x; i < (long long)G.Nc * T2_K; i += blockDim.x) {
+        const int cell = (int)(i / T2_K), l = (int)(i % T2_K);
+        float x = 0.f;
+        if (l < P) {
+            x = v < G.nvdf ? (float)(G.f[(size_t)v * G.N + (size_t)cell * P + l] * sc) : 0.f;
+            G.F[(((size_t)bt * G.Nc + cell) * P + l) * G.VB + lb] = x;
+        }
         const __half h = __float2half_rn(x);
         const __half lo = __float2half_rn(x - __half2float(h));
-        unsigned char *base = F16 + ((size_t)(2 * bt) * Nc + cell) * tile + t2_off(v, l);
+        unsigned char *base = G.F16 + ((size_t)(2 * bt) * G.Nc + cell) * tile + t2_off(lb, l);
         *reinterpret_cast<__half *>(base) = h;
-        *reinterpret_cast<__half *>(base + (size_t)Nc * tile) = lo;
+        *reinterpret_cast<__half *>(base + (size_t)G.Nc * tile) = lo;
+    }
+}
+
+// q[v][i] = scale * 2 * qacc[i*NV + v] / w[i] for the grids of one launch
+struct Tc2FinalGrid {
+    const double *qacc, *w;
+    double *q;
+    long long N;
+    int nvdf, NV;
+    double scale;
+};
+struct Tc2FinalLaunch {
+    Tc2FinalGrid g[T2_MAXG];
+    int ngrids;
+    long long ebase[T2_MAXG + 1];  // first output element of each grid
+};
+
+__global__ void k_tc2_final(const __grid_constant__ Tc2FinalLaunch A)
+{
+    const long long tot = A.ebase[A.ngrids];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < tot;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int gi = 0;
+        while (gi + 1 < A.ngrids && idx >= A.ebase[gi + 1]) gi++;
+        const Tc2FinalGrid &G = A.g[gi];
+        const long long k = idx - A.ebase[gi];
+        const int v = (int)(k % G.nvdf);
+        const long long i = k / G.nvdf;
+        double val = 2.0 * G.qacc[i * G.NV + v] / G.w[i];
+        if (G.scale != 1.0) val = val * G.scale;
+        G.q[(size_t)v * G.N + i] = val;
     }
 }
 
@@ -931,7 +1009,6 @@ struct Tc2Args {
     int ng;      // row tiles
 };
 
-constexpr int T2_MAXG = 4;  // grids of one launch (mixed-grid batches)
 
 // One launch of the block form.  Its work is a sequence of units, unit
 // ubase[g] + (s*ng + t)*nbp + bp serving, for grid g, block set s, the t-th
@@ -1685,10 +1762,46 @@ static void tc2_use_tuned(Ctx *c, int nvdf)
 struct Tc2Call {
     Tc2Args a;
     TcLists tl;
+    Tc2PrepGrid prep;
     int VB = 0, region = 0;
 };
 
-static int tc2_begin(Ctx *c, const double *d_f, int nvdf, Tc2Call &k)
+// the f preparation of the grids of one launch (one CTA per VDF slot)
+static int tc2_launch_prep(Ctx *c, const Tc2PrepGrid *gs, int n, cudaStream_t stream)
+{
+    Tc2PrepLaunch A;
+    std::memset(&A, 0, sizeof(A));
+    A.ngrids = n;
+    for (int i = 0; i < n; i++) {
+        A.g[i] = gs[i];
+        A.vbase[i + 1] = A.vbase[i] + gs[i].NV;
+    }
+    k_tc2_prep<<<(unsigned)A.vbase[n], 256, 0, stream>>>(A);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 1);
+    return DGV_OK;
+}
+
+// the final step (FP64 sums / w x scale into q) of the grids of one launch
+static int tc2_launch_final(Ctx *c, const Tc2FinalGrid *gs, int n, cudaStream_t stream)
+{
+    Tc2FinalLaunch A;
+    std::memset(&A, 0, sizeof(A));
+    A.ngrids = n;
+    for (int i = 0; i < n; i++) {
+        A.g[i] = gs[i];
+        A.ebase[i + 1] = A.ebase[i] + (long long)gs[i].nvdf * gs[i].N;
+    }
+    const long long tot = A.ebase[n];
+    k_tc2_final<<<(unsigned)std::min<long long>((tot + 255) / 256, 148LL * 32), 256, 0, stream>>>(A);
+    DGV_CUDA(c, cudaGetLastError());
+    count_launches(c, 1);
+    return DGV_OK;
+}
+
+// launch_prep = false: the caller launches the f preparation (k.prep) with
+// those of other grids
+static int tc2_begin(Ctx *c, const double *d_f, int nvdf, Tc2Call &k, cudaStream_t stream, bool launch_prep)
 {
     const Grid &g = c->grid;
     Layout &L = c->lay;
@@ -1714,12 +1827,9 @@ static int tc2_begin(Ctx *c, const double *d_f, int nvdf, Tc2Call &k)
     float *F = reinterpret_cast<float *>(c->d_tcF);
     unsigned char *F16 = reinterpret_cast<unsigned char *>(c->d_tcF) + fbytes;
     double *inv = reinterpret_cast<double *>(F16 + f16bytes);
-    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc2_vscale, F, inv, g.Nc, g.P, VB, 2);
-    DGV_CUDA(c, cudaGetLastError());
-    k_tc2_f16<<<1184, 256, 0, c->stream>>>(F, F16, nbt, g.Nc, g.P, VB);
-    DGV_CUDA(c, cudaGetLastError());
-    DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, c->stream));
-    count_launches(c, 2);  // k_tc_fprep, k_tc2_f16
+    k.prep = Tc2PrepGrid{d_f, F, F16, inv, g.N, nvdf, NV, g.Nc, g.P, VB, 2, 1.0 / L.tc2_vscale};
+    DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, qbytes, stream));
+    if (launch_prep && (rc = tc2_launch_prep(c, &k.prep, 1, stream))) return rc;
     Tc2Args &a = k.a;
     std::memset(&a, 0, sizeof(a));
     a.F = F; a.F16 = F16; a.W = (const unsigned char *)L.tc2_W; a.W2 = nullptr; a.items = k.tl.items;
@@ -1736,13 +1846,16 @@ static int tc2_begin(Ctx *c, const double *d_f, int nvdf, Tc2Call &k)
     return ensure_buffer(c, &c->d_tc2done, &c->tc2done_bytes, t2_flag_bytes(a));
 }
 
+static Tc2FinalGrid tc2_final_of(Ctx *c, double *d_q, int nvdf, int NV, double scale)
+{
+    return Tc2FinalGrid{c->d_tcQ, c->d_nwt, d_q, c->grid.N, nvdf, NV, scale};
+}
+
 static int tc2_end(Ctx *c, double *d_q, int nvdf, int NV, double scale)
 {
-    const Grid &g = c->grid;
-    const long long tot = (long long)nvdf * g.N;
-    k_tc_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, c->d_nwt, d_q, g.N, nvdf, NV, scale);
-    DGV_CUDA(c, cudaGetLastError());
-    count_launches(c, 1);  // k_tc_final
+    const Tc2FinalGrid fg = tc2_final_of(c, d_q, nvdf, NV, scale);
+    int rc = tc2_launch_final(c, &fg, 1, c->stream);
+    if (rc) return rc;
     if (c->project) return project_device(c, d_q, nvdf);
     return DGV_OK;
 }
@@ -1750,7 +1863,7 @@ static int tc2_end(Ctx *c, double *d_q, int nvdf, int NV, double scale)
 static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, double scale)
 {
     Tc2Call k;
-    int rc = tc2_begin(c, d_f, nvdf, k);
+    int rc = tc2_begin(c, d_f, nvdf, k, c->stream, true);
     if (rc) return rc;
     const std::vector<int> &sets = c->lay.tc2_sets;
     rc = c->grid.P == 27 ? launch_tc2_vb<27>(c, k.a, k.tl, k.VB, sets, k.region)
@@ -1761,12 +1874,12 @@ static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, do
 
 // Mixed-grid batch (dgv_collide_group) in one persistent launch: members of
 // the block form with the same nodes per cell and VDF tile size (at most
-// T2_MAXG of them).  Each member's preparation runs on its own stream (after
-// `fork` on the origin stream), the launch on the origin stream serves every
-// member's units (grid after grid, each in set order with its own order
-// flags), then each member's final step on its stream; join[i] / join[n + i]
-// bring the members back to the origin.  The members' tuned launch choices
-// (VDF tiles per CTA, records per launch) are kept.
+// T2_MAXG of them).  On the origin stream: one launch prepares every
+// member's f tiles, the persistent launch serves every member's units (grid
+// after grid, each in set order with its own order flags), one launch writes
+// every member's Q; a member's conservation projection, if on, runs on its
+// own stream (after fork2; join[n + i] brings it back).  The members' tuned
+// launch choices (VDF tiles per CTA, records per launch) are kept.
 int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, const int *nb, int n,
                       cudaStream_t origin, cudaEvent_t fork, cudaEvent_t fork2, const cudaEvent_t *join)
 {
@@ -1795,16 +1908,16 @@ int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, 
         Lh.tpcmax = tpm;
     }
     tc2_wait_args(c0, Lh);
-    DGV_CUDA(c0, cudaEventRecord(fork, origin));
+    (void)fork;
     int units = 0;
     std::vector<int> NVs(n);
+    std::vector<Tc2PrepGrid> preps(n);
     for (int i = 0; i < n; i++) {
         Ctx *c = cs[i];
-        if (c->stream != origin) DGV_CUDA(c, cudaStreamWaitEvent(c->stream, fork, 0));
         Tc2Call k;
-        int rc = tc2_begin(c, f[i], nb[i], k);
+        int rc = tc2_begin(c, f[i], nb[i], k, origin, false);
         if (rc) return rc;
-        DGV_CUDA(c, cudaMemsetAsync(c->d_tc2done, 0, t2_flag_bytes(k.a), c->stream));
+        DGV_CUDA(c, cudaMemsetAsync(c->d_tc2done, 0, t2_flag_bytes(k.a), origin));
         k.a.item_start = k.tl.item_start;
         k.a.tile_of = k.tl.tile_of;
         k.a.done = reinterpret_cast<int *>(c->d_tc2done);
@@ -1814,10 +1927,11 @@ int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, 
         Lh.ubase[i] = units;
         units += ((int)c->lay.tc2_sets.size() - 1) * k.a.nbp * k.a.ng;
         NVs[i] = k.a.NV;
-        if (c->stream != origin) {
-            DGV_CUDA(c, cudaEventRecord(join[i], c->stream));
-            DGV_CUDA(c0, cudaStreamWaitEvent(origin, join[i], 0));
-        }
+        preps[i] = k.prep;
+    }
+    {
+        const int rc = tc2_launch_prep(c0, preps.data(), n, origin);
+        if (rc) return rc;
     }
     Lh.ubase[n] = units;
     int rc;
@@ -1842,11 +1956,16 @@ int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, 
     }
     if (rc) return rc;
     count_launches(c0, 1);
+    std::vector<Tc2FinalGrid> finals(n);
+    for (int i = 0; i < n; i++) finals[i] = tc2_final_of(cs[i], q[i], nb[i], NVs[i], 1.0);
+    if ((rc = tc2_launch_final(c0, finals.data(), n, origin))) return rc;
+    // each member's conservation projection, if it has it on, on its stream
     DGV_CUDA(c0, cudaEventRecord(fork2, origin));
     for (int i = 0; i < n; i++) {
         Ctx *c = cs[i];
+        if (!c->project) continue;
         if (c->stream != origin) DGV_CUDA(c, cudaStreamWaitEvent(c->stream, fork2, 0));
-        if ((rc = tc2_end(c, q[i], nb[i], NVs[i], 1.0))) return rc;
+        if ((rc = project_device(c, q[i], nb[i]))) return rc;
         if (c->stream != origin) {
             DGV_CUDA(c, cudaEventRecord(join[n + i], c->stream));
             DGV_CUDA(c0, cudaStreamWaitEvent(origin, join[n + i], 0));
@@ -2074,10 +2193,10 @@ static int vjp_tc_body(Ctx *c, const double *d_f, const double *d_v, double *d_g
     float *Cf = reinterpret_cast<float *>(F16 + f16bytes);
     double *inv_f = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(Cf) + fbytes);
     double *inv_c = inv_f + NV;
-    k_tc_fprep<<<NV, 256, 0, c->stream>>>(d_f, g.N, nvdf, 1.0 / L.tc2_vscale, F, inv_f, g.Nc, g.P, VB, 1);
-    DGV_CUDA(c, cudaGetLastError());
-    k_tc2_f16<<<1184, 256, 0, c->stream>>>(F, F16, nbt, g.Nc, g.P, VB);
-    DGV_CUDA(c, cudaGetLastError());
+    {
+        const Tc2PrepGrid pg{d_f, F, F16, inv_f, g.N, nvdf, NV, g.Nc, g.P, VB, 1, 1.0 / L.tc2_vscale};
+        if ((rc = tc2_launch_prep(c, &pg, 1, c->stream))) return rc;
+    }
     k_tc_cprep<<<NV, 256, 0, c->stream>>>(d_v, c->d_nwt, g.N, nvdf, Cf, inv_c, g.Nc, g.P, VB);
     DGV_CUDA(c, cudaGetLastError());
     DGV_CUDA(c, cudaMemsetAsync(c->d_tcQ, 0, gbytes, c->stream));
@@ -2096,7 +2215,7 @@ static int vjp_tc_body(Ctx *c, const double *d_f, const double *d_v, double *d_g
     const long long tot = (long long)nvdf * g.N;
     k_tc_vjp_final<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->d_tcQ, inv_f, inv_c, d_g, g.N, nvdf, NV);
     DGV_CUDA(c, cudaGetLastError());
-    count_launches(c, 4);  // k_tc_fprep, k_tc2_f16, k_tc_cprep, k_tc_vjp_final
+    count_launches(c, 2);  // k_tc_cprep, k_tc_vjp_final (k_tc2_prep counted above)
     return DGV_OK;
 }
 
