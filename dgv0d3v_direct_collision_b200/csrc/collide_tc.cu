@@ -1881,7 +1881,7 @@ static int collide_tc2_body(Ctx *c, const double *d_f, double *d_q, int nvdf, do
 // own stream (after fork2; join[n + i] brings it back).  The members' tuned
 // launch choices (VDF tiles per CTA, records per launch) are kept.
 int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, const int *nb, int n,
-                      cudaStream_t origin, cudaEvent_t fork, cudaEvent_t fork2, const cudaEvent_t *join)
+                      cudaStream_t origin, cudaEvent_t fork2, const cudaEvent_t *join)
 {
     Ctx *c0 = cs[0];
     if (n < 1 || n > T2_MAXG) return set_err(c0, DGV_EUNSUP, "collide_group: persistent launch serves 1-4 grids");
@@ -1908,7 +1908,6 @@ int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, 
         Lh.tpcmax = tpm;
     }
     tc2_wait_args(c0, Lh);
-    (void)fork;
     int units = 0;
     std::vector<int> NVs(n);
     std::vector<Tc2PrepGrid> preps(n);

@@ -9,8 +9,9 @@
 // second captures the whole fork/join into one CUDA graph; later calls replay
 // it with a single launch.  The members' kernels may overlap on the device.
 // On the tensor cores (block form, same nodes per cell and VDF tile size, at
-// most four members) the captured graph holds one persistent collision kernel
-// for all members instead of one launch per member and block set.
+// most four members) the captured graph holds three kernels for all members
+// -- the f preparation, one persistent collision kernel, the final step --
+// instead of several launches per member and block set.
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -22,7 +23,7 @@ namespace dgv {
 
 int collide_device(Ctx *c, const double *d_f, double *d_q, int nvdf, int precision, double scale);
 int collide_tc2_group(Ctx *const *cs, const double *const *f, double *const *q, const int *nb, int n,
-                      cudaStream_t origin, cudaEvent_t fork, cudaEvent_t fork2, const cudaEvent_t *join);
+                      cudaStream_t origin, cudaEvent_t fork2, const cudaEvent_t *join);
 
 namespace {
 
@@ -78,7 +79,7 @@ int run_members(const GroupKey &k, cudaEvent_t fork, cudaEvent_t fork2, std::vec
         }
         if (proj_ok) {
             const int rc = collide_tc2_group(cs.data(), fs.data(), qs.data(), nbs.data(), (int)cs.size(), k.origin,
-                                             fork, fork2, join.data());
+                                             fork2, join.data());
             if (rc != DGV_EUNSUP) return rc;
             c0->err.clear();  // members that cannot share a launch: one call per member
         }
