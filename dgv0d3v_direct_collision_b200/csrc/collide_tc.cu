@@ -1451,7 +1451,12 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                     if (lane == 0) mbar_arrive(&c_empty[cs]);
                 }
                 if (!ok) break;
+                Jb += ngb * nb2;
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
                 if constexpr (MODE == 1) {
+                    // after the slot is released: the node totals come from
+                    // registers and local memory only
                     if (valid) {
 #pragma unroll
                         for (int p = 0; p < P; p++) {  // two-sum of the node totals into (sum, correction)
@@ -1463,9 +1468,6 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                         }
                     }
                 }
-                Jb += ngb * nb2;
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&s_empty[s]);  // this warp's reads of the slot are done
                 if constexpr (MODE == 0) {
                     // the item's total two-summed into (sum, correction); a row the
                     // item does not serve adds exact zeros (zero side factors)
