@@ -1368,12 +1368,20 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                 i1 = un.i1;
                 err = L.g[MG ? un.gi : 0].err;
             }
-            float S[P], Cc[P];
+            // (sum, correction) per node: MODE 1 one float each; MODE 0 nodes
+            // (2i, 2i+1) in the halves of one float2, so that the item fold
+            // runs in packed FP32x2 operations
+            constexpr int P2 = (P + 1) / 2;
+            float S[MODE == 1 ? P : 1], Cc[MODE == 1 ? P : 1];
+            float2 S2[MODE == 0 ? P2 : 1], Cc2[MODE == 0 ? P2 : 1], acc2[MODE == 0 ? P2 : 1];
 #pragma unroll
-            for (int p = 0; p < P; p++) { S[p] = 0.f; Cc[p] = 0.f; }
-            float acc[MODE == 0 ? P : 1];  // MODE 0: the item's FP32 sums
+            for (int p = 0; p < (MODE == 1 ? P : 1); p++) { S[p] = 0.f; Cc[p] = 0.f; }
 #pragma unroll
-            for (int p = 0; p < (MODE == 0 ? P : 1); p++) acc[p] = 0.f;
+            for (int i = 0; i < (MODE == 0 ? P2 : 1); i++) {
+                S2[i] = make_float2(0.f, 0.f);
+                Cc2[i] = make_float2(0.f, 0.f);
+                acc2[i] = make_float2(0.f, 0.f);  // MODE 0: the item's FP32 sums
+            }
             for (int it = i0; it < i1; it++) {
                 const int s = q & 1;
                 if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, err, L.wait_ns)) { ok = false; break; }
@@ -1430,7 +1438,8 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                             const int n = g * T2_N + LW * hh + i;
                             if (n < P * P) {
                                 if constexpr (MODE == 0) {
-                                    acc[n % P] = fmaf(f1[n / P], __uint_as_float(G[i]), acc[n % P]);
+                                    float &a = ((n % P) & 1) ? acc2[(n % P) / 2].y : acc2[(n % P) / 2].x;
+                                    a = fmaf(f1[n / P], __uint_as_float(G[i]), a);
                                 } else {
                                     // NR interleaved partial sums over p
                                     const int pp = n % P, rr = pp % NR;
@@ -1469,14 +1478,23 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                     }
                 }
                 if constexpr (MODE == 0) {
-                    // the item's total two-summed into (sum, correction); a row the
-                    // item does not serve adds exact zeros (zero side factors)
+                    // the item's total two-summed into (sum, correction), two
+                    // nodes per packed operation: each half rounds like the
+                    // scalar operation, x - y is fma(y, -1, x) (one rounding,
+                    // as the subtraction), so the results are those of the
+                    // scalar two-sum; a row the item does not serve adds exact
+                    // zeros (zero side factors)
+                    const float2 m1 = make_float2(-1.f, -1.f);
 #pragma unroll
-                    for (int p = 0; p < P; p++) {
-                        const float t = S[p] + acc[p], bpv = t - S[p];
-                        Cc[p] += (S[p] - (t - bpv)) + (acc[p] - bpv);
-                        S[p] = t;
-                        acc[p] = 0.f;
+                    for (int i = 0; i < P2; i++) {
+                        const float2 x = acc2[i];
+                        const float2 t = __fadd2_rn(S2[i], x);
+                        const float2 bpv = __ffma2_rn(S2[i], m1, t);                       // t - S
+                        const float2 e1 = __ffma2_rn(__ffma2_rn(bpv, m1, t), m1, S2[i]);  // S - (t - bpv)
+                        const float2 e2 = __ffma2_rn(bpv, m1, x);                          // x - bpv
+                        Cc2[i] = __fadd2_rn(Cc2[i], __fadd2_rn(e1, e2));
+                        S2[i] = t;
+                        acc2[i] = make_float2(0.f, 0.f);
                     }
                 }
                 q++;
@@ -1498,7 +1516,15 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
 #pragma unroll
                 for (int p = 0; p < P; p++) {
                     double *dst = a.qacc + ((size_t)D * P + p) * a.NV + vdf;
-                    *dst += ((double)S[p] + (double)Cc[p]) * sc;
+                    float sv, cv;
+                    if constexpr (MODE == 0) {
+                        sv = (p & 1) ? S2[p / 2].y : S2[p / 2].x;
+                        cv = (p & 1) ? Cc2[p / 2].y : Cc2[p / 2].x;
+                    } else {
+                        sv = S[p];
+                        cv = Cc[p];
+                    }
+                    *dst += ((double)sv + (double)cv) * sc;
                 }
             }
             if (flag) {
