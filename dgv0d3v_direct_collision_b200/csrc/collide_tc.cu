@@ -1097,6 +1097,21 @@ __device__ __forceinline__ bool flag_wait(const int *flag, int target, int *err,
     return true;
 }
 
+// two-sum of x into (S, Cc), two nodes per packed operation: each half rounds
+// like the scalar operation and x - y is fma(y, -1, x) (one rounding, as the
+// subtraction), so the results are those of the scalar two-sum; x = 0 leaves
+// (S, Cc) unchanged
+__device__ __forceinline__ void two_sum2(float2 &S, float2 &Cc, float2 x)
+{
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 t = __fadd2_rn(S, x);
+    const float2 bpv = __ffma2_rn(S, m1, t);                       // t - S
+    const float2 e1 = __ffma2_rn(__ffma2_rn(bpv, m1, t), m1, S);  // S - (t - bpv)
+    const float2 e2 = __ffma2_rn(bpv, m1, x);                      // x - bpv
+    Cc = __fadd2_rn(Cc, __fadd2_rn(e1, e2));
+    S = t;
+}
+
 // MODE 0: Q(f,f), a CTA owns output cells D and an item (block c1, c2) reads
 //         F16 tiles of cells c2 + D and the FP32 side tile of cells c1 + D;
 //         per row acc[p] += f(c1+D, l1) G[(l1, p)].
@@ -1368,20 +1383,17 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                 i1 = un.i1;
                 err = L.g[MG ? un.gi : 0].err;
             }
-            // (sum, correction) per node: MODE 1 one float each; MODE 0 nodes
-            // (2i, 2i+1) in the halves of one float2, so that the item fold
-            // runs in packed FP32x2 operations
+            // (sum, correction) per node, nodes (2i, 2i+1) in the halves of one
+            // float2, so that the item folds run in packed FP32x2 operations
             constexpr int P2 = (P + 1) / 2;
-            float S[MODE == 1 ? P : 1], Cc[MODE == 1 ? P : 1];
-            float2 S2[MODE == 0 ? P2 : 1], Cc2[MODE == 0 ? P2 : 1], acc2[MODE == 0 ? P2 : 1];
+            float2 S2[P2], Cc2[P2], acc2[MODE == 0 ? P2 : 1];
 #pragma unroll
-            for (int p = 0; p < (MODE == 1 ? P : 1); p++) { S[p] = 0.f; Cc[p] = 0.f; }
-#pragma unroll
-            for (int i = 0; i < (MODE == 0 ? P2 : 1); i++) {
+            for (int i = 0; i < P2; i++) {
                 S2[i] = make_float2(0.f, 0.f);
                 Cc2[i] = make_float2(0.f, 0.f);
-                acc2[i] = make_float2(0.f, 0.f);  // MODE 0: the item's FP32 sums
             }
+#pragma unroll
+            for (int i = 0; i < (MODE == 0 ? P2 : 1); i++) acc2[i] = make_float2(0.f, 0.f);  // MODE 0: the item's sums
             for (int it = i0; it < i1; it++) {
                 const int s = q & 1;
                 if (!mbar_wait_warp(&s_full[s], (q >> 1) & 1, err, L.wait_ns)) { ok = false; break; }
@@ -1467,33 +1479,26 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
                     // after the slot is released: the node totals come from
                     // registers and local memory only
                     if (valid) {
+                        // two-sum of the node totals into (sum, correction);
+                        // nodes outside the mask add exact zeros
 #pragma unroll
-                        for (int p = 0; p < P; p++) {  // two-sum of the node totals into (sum, correction)
-                            if (!((msk >> p) & 1u)) continue;
-                            const float x = stg[__popc(msk & ((1u << p) - 1u))];
-                            const float t = S[p] + x, bpv = t - S[p];
-                            Cc[p] += (S[p] - (t - bpv)) + (x - bpv);
-                            S[p] = t;
+                        for (int i = 0; i < P2; i++) {
+                            float x[2];
+#pragma unroll
+                            for (int e = 0; e < 2; e++) {
+                                const int p = 2 * i + e;
+                                x[e] = (p < P && ((msk >> p) & 1u)) ? stg[__popc(msk & ((1u << p) - 1u))] : 0.f;
+                            }
+                            two_sum2(S2[i], Cc2[i], make_float2(x[0], x[1]));
                         }
                     }
                 }
                 if constexpr (MODE == 0) {
-                    // the item's total two-summed into (sum, correction), two
-                    // nodes per packed operation: each half rounds like the
-                    // scalar operation, x - y is fma(y, -1, x) (one rounding,
-                    // as the subtraction), so the results are those of the
-                    // scalar two-sum; a row the item does not serve adds exact
-                    // zeros (zero side factors)
-                    const float2 m1 = make_float2(-1.f, -1.f);
+                    // the item's total two-summed into (sum, correction); a row
+                    // the item does not serve adds exact zeros (zero side factors)
 #pragma unroll
                     for (int i = 0; i < P2; i++) {
-                        const float2 x = acc2[i];
-                        const float2 t = __fadd2_rn(S2[i], x);
-                        const float2 bpv = __ffma2_rn(S2[i], m1, t);                       // t - S
-                        const float2 e1 = __ffma2_rn(__ffma2_rn(bpv, m1, t), m1, S2[i]);  // S - (t - bpv)
-                        const float2 e2 = __ffma2_rn(bpv, m1, x);                          // x - bpv
-                        Cc2[i] = __fadd2_rn(Cc2[i], __fadd2_rn(e1, e2));
-                        S2[i] = t;
+                        two_sum2(S2[i], Cc2[i], acc2[i]);
                         acc2[i] = make_float2(0.f, 0.f);
                     }
                 }
@@ -1516,14 +1521,7 @@ __global__ void __launch_bounds__(T2_THREADS, 1) k_collide_tc2(const __grid_cons
 #pragma unroll
                 for (int p = 0; p < P; p++) {
                     double *dst = a.qacc + ((size_t)D * P + p) * a.NV + vdf;
-                    float sv, cv;
-                    if constexpr (MODE == 0) {
-                        sv = (p & 1) ? S2[p / 2].y : S2[p / 2].x;
-                        cv = (p & 1) ? Cc2[p / 2].y : Cc2[p / 2].x;
-                    } else {
-                        sv = S[p];
-                        cv = Cc[p];
-                    }
+                    const float sv = (p & 1) ? S2[p / 2].y : S2[p / 2].x, cv = (p & 1) ? Cc2[p / 2].y : Cc2[p / 2].x;
                     *dst += ((double)sv + (double)cv) * sc;
                 }
             }
